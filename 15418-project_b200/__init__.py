@@ -1,0 +1,284 @@
+"""gpjson_b200: Python host-side mirror of the reference's engine API.
+
+Thin ctypes bindings over the C ABI in include/gpjson_b200.h.  The names,
+argument meaning and errors follow the reference's C++ interface
+(Xinyu-Li-123/15418-project):
+
+  compile(query)               query::QueryCompiler::compile
+  Context.build_index(...)     index::IndexBuilder::build
+  Context.query(...)           query::QueryExecutor::execute_batch (device part)
+  Context.query_host(...)      the per-partition body of gpjson::Engine::query
+
+Device memory is passed as integer device pointers (for example
+torch.Tensor.data_ptr()); streams as integer cudaStream_t handles.  The native
+library is required: there is no CPU path, and loading fails loudly if the
+library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "lib" / "libgpjson_b200.so"
+
+GPJ_OK = 0
+GPJ_ERR_CUDA = 1
+GPJ_ERR_OOM = 2
+GPJ_ERR_MALFORMED_QUERY = 3
+GPJ_ERR_UNSUPPORTED_QUERY = 4
+GPJ_ERR_EXECUTION = 5
+GPJ_ERR_TIMEOUT = 6
+GPJ_ERR_INVALID_ARGUMENT = 7
+GPJ_ERR_OUT_OF_RANGE = 8
+GPJ_ERR_CAPACITY = 9
+GPJ_ERR_IMPLEMENTATION = 10
+
+GPJ_INDEX_EMIT_ESCAPE_QUOTE = 1
+GPJ_INDEX_NO_TMA = 2
+MAX_LEVELS = 22
+MAX_QUERY_IR = 4096
+MAX_QUERY_DEPTH = 16
+
+EXPORTED_SYMBOLS = (
+    "gpj_version", "gpj_last_error", "gpj_ctx_create", "gpj_ctx_destroy",
+    "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_free",
+    "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
+)
+
+
+# Exception hierarchy of the reference (include/gpjson/error/*.hpp).
+class GpJSONError(Exception):
+    pass
+
+
+class CudaError(GpJSONError):
+    pass
+
+
+class MalformedQueryError(GpJSONError):
+    pass
+
+
+class UnsupportedQueryError(GpJSONError):
+    pass
+
+
+class QueryExecutionError(GpJSONError):
+    pass
+
+
+class ImplementationError(GpJSONError):
+    pass
+
+
+class DeviceTimeoutError(GpJSONError):
+    """A bounded device-side wait gave up (no reference counterpart)."""
+
+
+class CapacityError(GpJSONError):
+    """A caller-provided buffer is too small (no reference counterpart)."""
+
+
+_ERRORS = {
+    GPJ_ERR_CUDA: CudaError,
+    GPJ_ERR_OOM: CudaError,
+    GPJ_ERR_MALFORMED_QUERY: MalformedQueryError,
+    GPJ_ERR_UNSUPPORTED_QUERY: UnsupportedQueryError,
+    GPJ_ERR_EXECUTION: QueryExecutionError,
+    GPJ_ERR_TIMEOUT: DeviceTimeoutError,
+    GPJ_ERR_INVALID_ARGUMENT: ValueError,
+    GPJ_ERR_OUT_OF_RANGE: OverflowError,
+    GPJ_ERR_CAPACITY: CapacityError,
+    GPJ_ERR_IMPLEMENTATION: ImplementationError,
+}
+
+
+class QueryOpts(C.Structure):
+    """gpj_query_opts."""
+
+    _fields_ = [("base_level", C.c_uint32), ("offset_bytes", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+
+class Index(C.Structure):
+    """gpj_index: device-resident structural indexes of one partition."""
+
+    _fields_ = [
+        ("d_input", C.c_void_p),
+        ("size_bytes", C.c_uint64),
+        ("d_newline", C.c_void_p),
+        ("num_lines", C.c_uint64),
+        ("newline_capacity", C.c_uint64),
+        ("d_string", C.c_void_p),
+        ("d_leveled", C.c_void_p),
+        ("d_escape", C.c_void_p),
+        ("d_quote", C.c_void_p),
+        ("num_words", C.c_uint64),
+        ("num_levels", C.c_int32),
+        ("final_in_string", C.c_int32),
+        ("final_depth", C.c_int32),
+        ("reserved", C.c_int32),
+        ("owner", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def library_path() -> Path:
+    return LIB_PATH
+
+
+def load_library(build_if_missing: bool = False) -> C.CDLL:
+    """Loads libgpjson_b200.so; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        if not build_if_missing:
+            raise RuntimeError(
+                f"native library {LIB_PATH} is missing: build it first "
+                "(python __graft_entry__.py or 15418-project_b200/build.py)")
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("_gpjb_build", _PKG / "build.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build_library()
+    lib = C.CDLL(str(LIB_PATH))
+    u64, u32, vp, i32 = C.c_uint64, C.c_uint32, C.c_void_p, C.c_int
+    P = C.POINTER
+    lib.gpj_version.restype = i32
+    lib.gpj_last_error.restype = C.c_char_p
+    lib.gpj_ctx_create.argtypes = [i32, P(vp)]
+    lib.gpj_ctx_destroy.argtypes = [vp]
+    lib.gpj_compile.argtypes = [C.c_char_p, u64, vp, u64, P(u64), P(u64), P(u64)]
+    lib.gpj_index_build.argtypes = [vp, vp, u64, i32, u32, P(Index), vp]
+    lib.gpj_index_build_async.argtypes = [vp, vp, u64, i32, u32, P(Index), vp, vp]
+    lib.gpj_index_free.argtypes = [vp, P(Index)]
+    lib.gpj_query_run.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
+    lib.gpj_query_run64.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
+    lib.gpj_query_run_opts.argtypes = [vp, P(Index), vp, u64, u32, P(QueryOpts), vp, vp]
+    lib.gpj_query_host.argtypes = [vp, vp, u64, i32, u32, vp, vp, vp, vp, vp, vp, P(u64), vp]
+    for name in EXPORTED_SYMBOLS:
+        if name != "gpj_version" and name != "gpj_last_error":
+            getattr(lib, name).restype = i32
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != GPJ_OK:
+        msg = load_library().gpj_last_error().decode(errors="replace")
+        raise _ERRORS.get(rc, GpJSONError)(msg)
+
+
+@dataclass(frozen=True)
+class CompiledQuery:
+    """query::CompiledQuery (include/gpjson/query/query.hpp:23-43)."""
+
+    query_text: str
+    ir_bytes: bytes
+    max_depth: int
+    num_result_slots: int
+
+
+def compile(query: str, wildcard_limit: int = 0) -> CompiledQuery:  # noqa: A001
+    """Compiles a JSONPath query (query_compiler.cpp QueryParser::compile)."""
+    lib = load_library()
+    n, depth, slots = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    cap = MAX_QUERY_IR
+    while True:
+        buf = (C.c_uint8 * cap)()
+        rc = lib.gpj_compile(query.encode(), wildcard_limit, buf, cap, C.byref(n),
+                             C.byref(depth), C.byref(slots))
+        if rc == GPJ_ERR_CAPACITY and n.value > cap:
+            cap = n.value
+            continue
+        _check(rc)
+        break
+    return CompiledQuery(query, bytes(buf[: n.value]), depth.value, slots.value)
+
+
+class Context:
+    """A device binding plus reusable device buffers (gpj_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        _check(self._lib.gpj_ctx_create(device, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.gpj_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def build_index(self, d_input: int, size_bytes: int, num_levels: int,
+                    flags: int = 0, stream: int = 0) -> Index:
+        ix = Index()
+        _check(self._lib.gpj_index_build(self._h, C.c_void_p(d_input), size_bytes,
+                                         num_levels, flags, C.byref(ix),
+                                         C.c_void_p(stream)))
+        return ix
+
+    def build_index_async(self, d_input: int, size_bytes: int, num_levels: int,
+                          index: Index, d_summary: int, flags: int = 0,
+                          stream: int = 0) -> None:
+        _check(self._lib.gpj_index_build_async(self._h, C.c_void_p(d_input), size_bytes,
+                                               num_levels, flags, C.byref(index),
+                                               C.c_void_p(d_summary), C.c_void_p(stream)))
+
+    def free_index(self, index: Index) -> None:
+        _check(self._lib.gpj_index_free(self._h, C.byref(index)))
+
+    def query(self, index: Index, compiled: CompiledQuery, d_out: int, stream: int = 0,
+              wide: bool = False, base_level: int = 0) -> None:
+        ir = (C.c_uint8 * max(1, len(compiled.ir_bytes))).from_buffer_copy(
+            compiled.ir_bytes or b"\0")
+        if base_level == 0:
+            fn = self._lib.gpj_query_run64 if wide else self._lib.gpj_query_run
+            _check(fn(self._h, C.byref(index), ir, len(compiled.ir_bytes),
+                      compiled.num_result_slots, C.c_void_p(d_out), C.c_void_p(stream)))
+            return
+        opts = QueryOpts(base_level, 8 if wide else 4)
+        _check(self._lib.gpj_query_run_opts(self._h, C.byref(index), ir, len(compiled.ir_bytes),
+                                            compiled.num_result_slots, C.byref(opts),
+                                            C.c_void_p(d_out), C.c_void_p(stream)))
+
+    def query_host(self, h_input: int, size_bytes: int, num_levels: int,
+                   compiled: list[CompiledQuery], h_outs: list[int],
+                   capacities: list[int], stream: int = 0,
+                   base_levels: list[int] | None = None) -> int:
+        """Host in, host out: returns the number of records."""
+        q = len(compiled)
+        irs = [(C.c_uint8 * max(1, len(c.ir_bytes))).from_buffer_copy(c.ir_bytes or b"\0")
+               for c in compiled]
+        ir_ptrs = (C.c_void_p * max(1, q))(*[C.addressof(b) for b in irs])
+        ir_lens = (C.c_uint64 * max(1, q))(*[len(c.ir_bytes) for c in compiled])
+        slots = (C.c_uint32 * max(1, q))(*[c.num_result_slots for c in compiled])
+        outs = (C.c_void_p * max(1, q))(*h_outs)
+        caps = (C.c_uint64 * max(1, q))(*capacities)
+        bases = (C.c_uint32 * max(1, q))(*(base_levels or [0] * q))
+        lines = C.c_uint64()
+        _check(self._lib.gpj_query_host(self._h, C.c_void_p(h_input), size_bytes, num_levels,
+                                        q, ir_ptrs, ir_lens, slots, bases, outs, caps,
+                                        C.byref(lines), C.c_void_p(stream)))
+        return lines.value

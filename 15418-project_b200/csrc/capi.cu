@@ -1,0 +1,485 @@
+// C ABI of the engine (include/gpjson_b200.h): argument checks, device
+// buffer reuse, launches and error reporting.  No CPU fallback: every entry
+// point that computes needs a CUDA device and fails with GPJ_ERR_CUDA
+// otherwise.
+#include "compiler.hpp"
+#include "indexer.cuh"
+#include "query.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+
+struct gpj_ctx {
+  int device = 0;
+  // grow-only device buffers
+  void *scratch = nullptr;
+  uint64_t scratch_bytes = 0;
+  void *staging = nullptr;  // aligned copy of unaligned inputs / host inputs
+  uint64_t staging_bytes = 0;
+  // host_query(): index + results kept between calls
+  void *host_index = nullptr;
+  uint64_t host_index_bytes = 0;
+  void *host_results = nullptr;
+  uint64_t host_results_bytes = 0;
+  unsigned long long *pinned = nullptr;  // 8 words of pinned host memory
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  (void)cudaGetLastError();
+  const int code = (e == cudaErrorMemoryAllocation) ? GPJ_ERR_OOM : GPJ_ERR_CUDA;
+  return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GPJ_CUDA(call, what)                      \
+  do {                                            \
+    const cudaError_t e_ = (call);                \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+int ensure(void *&buf, uint64_t &have, uint64_t need) {
+  if (need <= have && buf != nullptr) return GPJ_OK;
+  if (buf != nullptr) {
+    cudaFree(buf);
+    buf = nullptr;
+    have = 0;
+  }
+  if (need == 0) need = 256;
+  GPJ_CUDA(cudaMalloc(&buf, need), "cudaMalloc");
+  have = need;
+  return GPJ_OK;
+}
+
+int bind_device(gpj_ctx *ctx) {
+  if (ctx == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null context");
+  GPJ_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  return GPJ_OK;
+}
+
+uint64_t round256(uint64_t x) { return (x + 255u) & ~uint64_t(255); }
+
+// Newline-index capacity guess for a fresh build: one record per 32 bytes
+// covers every realistic JSON-lines file; a build that finds more newlines
+// is repeated with the exact size.
+uint64_t nl_capacity_guess(uint64_t n) { return n / 32u + 1024u; }
+
+// Enqueues the fused indexer.  `in` may be unaligned: it is then copied into
+// the context's staging buffer first (TMA needs 16-byte aligned rows).
+int enqueue_index(gpj_ctx *ctx, const uint8_t *in, uint64_t n, int levels,
+                  uint32_t flags, const gpj_index &out, cudaStream_t stream) {
+  gpjb::IndexLaunch L;
+  L.n = n;
+  L.W = (n + 63u) / 64u;
+  L.num_levels = levels;
+  L.full_rows = n / 128u;
+  L.S = out.d_string;
+  L.LB = out.d_leveled;
+  L.E = (flags & GPJ_INDEX_EMIT_ESCAPE_QUOTE) ? out.d_escape : nullptr;
+  L.Q = (flags & GPJ_INDEX_EMIT_ESCAPE_QUOTE) ? out.d_quote : nullptr;
+  L.NL = out.d_newline;
+  L.nl_cap = out.newline_capacity;
+  L.num_tiles = uint32_t(gpjb::index_num_tiles(n));
+
+  const uint8_t *src = in;
+  if (n > 0 && (reinterpret_cast<uintptr_t>(in) & 15u) != 0) {
+    int rc = ensure(ctx->staging, ctx->staging_bytes, round256(n));
+    if (rc != GPJ_OK) return rc;
+    GPJ_CUDA(cudaMemcpyAsync(ctx->staging, in, n, cudaMemcpyDeviceToDevice, stream),
+             "copy unaligned input");
+    src = static_cast<const uint8_t *>(ctx->staging);
+  }
+  L.in = src;
+
+  int rc = ensure(ctx->scratch, ctx->scratch_bytes, gpjb::index_scratch_bytes(n));
+  if (rc != GPJ_OK) return rc;
+  gpjb::index_bind_scratch(L, ctx->scratch);
+
+  CUtensorMap map;
+  bool tma = false;
+  if ((flags & GPJ_INDEX_NO_TMA) == 0) tma = gpjb::index_make_tensor_map(&map, src, n);
+  if (n == 0) {
+    // no tiles: NL = [0], one line, empty bitmaps; the summary is written
+    // here because no kernel runs
+    const unsigned long long summary[4] = {1ull, 0ull, ~0ull, 0ull};
+    GPJ_CUDA(cudaMemsetAsync(ctx->scratch, 0, 64, stream), "cudaMemsetAsync");
+    GPJ_CUDA(cudaMemcpyAsync(L.summary, summary, sizeof(summary), cudaMemcpyHostToDevice,
+                             stream),
+             "summary");
+    if (out.newline_capacity > 0)
+      GPJ_CUDA(cudaMemsetAsync(out.d_newline, 0, sizeof(int64_t), stream), "cudaMemsetAsync");
+    return GPJ_OK;
+  }
+  GPJ_CUDA(gpjb::index_launch(L, tma ? &map : nullptr, tma, stream), "index kernel launch");
+  return GPJ_OK;
+}
+
+// summary words in the context scratch: [lines, in_string, depth, pad] then
+// the error word
+const unsigned long long *summary_ptr(gpj_ctx *ctx, uint64_t n) {
+  gpjb::IndexLaunch L;
+  L.num_tiles = uint32_t(gpjb::index_num_tiles(n));
+  gpjb::index_bind_scratch(L, ctx->scratch);
+  return L.summary;
+}
+const unsigned int *error_ptr(gpj_ctx *ctx, uint64_t n) {
+  gpjb::IndexLaunch L;
+  L.num_tiles = uint32_t(gpjb::index_num_tiles(n));
+  gpjb::index_bind_scratch(L, ctx->scratch);
+  return L.error;
+}
+
+// Copies the summary and error word to pinned memory and waits.
+int read_summary(gpj_ctx *ctx, uint64_t n, cudaStream_t stream, uint64_t *lines,
+                 int *in_string, int *depth) {
+  GPJ_CUDA(cudaMemcpyAsync(ctx->pinned, summary_ptr(ctx, n), 32, cudaMemcpyDeviceToHost,
+                           stream),
+           "read index summary");
+  GPJ_CUDA(cudaMemcpyAsync(ctx->pinned + 4, error_ptr(ctx, n), 4, cudaMemcpyDeviceToHost,
+                           stream),
+           "read index error word");
+  GPJ_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+  const unsigned int err = reinterpret_cast<const unsigned int *>(ctx->pinned + 4)[0];
+  if (n > 0 && err != 0)
+    return fail(GPJ_ERR_TIMEOUT, "index kernel: a bounded wait gave up (error bits " +
+                                     std::to_string(err) + ")");
+  *lines = ctx->pinned[0];
+  *in_string = int(ctx->pinned[1]);
+  *depth = int(int64_t(ctx->pinned[2]));
+  return GPJ_OK;
+}
+
+void release_index(gpj_index *ix) {
+  if (ix->owner != nullptr) cudaFree(ix->owner);
+  std::memset(ix, 0, sizeof(*ix));
+}
+
+// Carves one allocation into the index arrays.
+int alloc_index(gpj_index *ix, uint64_t n, int levels, bool eq, uint64_t nl_cap) {
+  const uint64_t W = (n + 63u) / 64u;
+  const uint64_t s_bytes = round256(W * 8u);
+  const uint64_t lb_bytes = round256(W * 8u * uint64_t(levels));
+  const uint64_t nl_bytes = round256(nl_cap * 8u);
+  const uint64_t eq_bytes = eq ? 2u * s_bytes : 0u;
+  void *mem = nullptr;
+  GPJ_CUDA(cudaMalloc(&mem, s_bytes + lb_bytes + nl_bytes + eq_bytes + 256u), "cudaMalloc index");
+  auto *p = static_cast<unsigned char *>(mem);
+  ix->owner = mem;
+  ix->d_string = reinterpret_cast<uint64_t *>(p);
+  ix->d_leveled = reinterpret_cast<uint64_t *>(p + s_bytes);
+  ix->d_newline = reinterpret_cast<int64_t *>(p + s_bytes + lb_bytes);
+  ix->newline_capacity = nl_cap;
+  if (eq) {
+    ix->d_escape = reinterpret_cast<uint64_t *>(p + s_bytes + lb_bytes + nl_bytes);
+    ix->d_quote = reinterpret_cast<uint64_t *>(p + s_bytes + lb_bytes + nl_bytes + s_bytes);
+  } else {
+    ix->d_escape = nullptr;
+    ix->d_quote = nullptr;
+  }
+  ix->num_words = W;
+  ix->num_levels = levels;
+  return GPJ_OK;
+}
+
+int check_levels(int levels) {
+  if (levels < 0 || levels > GPJ_MAX_LEVELS)
+    return fail(GPJ_ERR_INVALID_ARGUMENT,
+                "num_levels must be in [0, " + std::to_string(GPJ_MAX_LEVELS) + "]");
+  return GPJ_OK;
+}
+
+template <typename OutT>
+int run_query(gpj_ctx *ctx, const gpj_index *ix, const uint8_t *h_ir, uint64_t ir_len,
+              uint32_t slots, OutT *d_out, cudaStream_t stream, uint32_t base_level = 0) {
+  if (ix == nullptr || d_out == nullptr || h_ir == nullptr)
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "null argument");
+  if (ir_len > uint64_t(GPJ_MAX_QUERY_IR))
+    return fail(GPJ_ERR_EXECUTION, "Compiled query IR exceeds constant memory buffer");
+  if (ix->num_lines == 0 || ix->size_bytes == 0) return GPJ_OK;
+  if (ix->num_lines > ix->newline_capacity)
+    return fail(GPJ_ERR_CAPACITY, "newline index was truncated: rebuild with capacity >= " +
+                                      std::to_string(ix->num_lines));
+  if (base_level > 0 && int64_t(base_level) >= int64_t(ix->num_levels))
+    return fail(GPJ_ERR_EXECUTION, "Query requires more bitmap levels than the index provides");
+  if (sizeof(OutT) == 4 && ix->size_bytes > 0x7FFFFFFFull)
+    return fail(GPJ_ERR_EXECUTION, "partition size exceeds CUDA int range");
+  int rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  gpjb::QueryLaunch q;
+  q.in = ix->d_input;
+  q.n = int64_t(ix->size_bytes);
+  q.NL = ix->d_newline;
+  q.num_lines = int64_t(ix->num_lines);
+  q.S = ix->d_string;
+  q.LB = ix->d_leveled;
+  q.W = int64_t(ix->num_words);
+  q.ir_len = int(ir_len);
+  q.num_results = int(slots);
+  q.base_level = int(base_level);
+  q.num_levels = ix->num_levels;
+  if constexpr (sizeof(OutT) == 8) q.out64 = reinterpret_cast<int64_t *>(d_out);
+  else q.out32 = reinterpret_cast<int32_t *>(d_out);
+  gpjb::IrBlob blob;
+  std::memset(blob.bytes, 0, sizeof(blob.bytes));
+  std::memcpy(blob.bytes, h_ir, size_t(ir_len));
+  GPJ_CUDA(gpjb::query_launch(q, blob, 0, 256, stream), "query kernel launch");
+  return GPJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpj_version(void) { return 100; }
+
+const char *gpj_last_error(void) { return g_error.c_str(); }
+
+int gpj_ctx_create(int device, gpj_ctx **out) {
+  if (out == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null output");
+  *out = nullptr;
+  int count = 0;
+  const cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(GPJ_ERR_CUDA, "no CUDA device: the B200 engine has no CPU path");
+  if (device < 0 || device >= count) return fail(GPJ_ERR_INVALID_ARGUMENT, "bad device");
+  GPJ_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  gpj_ctx *ctx = new (std::nothrow) gpj_ctx;
+  if (ctx == nullptr) return fail(GPJ_ERR_OOM, "host allocation");
+  ctx->device = device;
+  void *pinned = nullptr;
+  const cudaError_t pe = cudaMallocHost(&pinned, 64);
+  if (pe != cudaSuccess) {
+    delete ctx;
+    return cuda_fail(pe, "cudaMallocHost");
+  }
+  ctx->pinned = static_cast<unsigned long long *>(pinned);
+  *out = ctx;
+  return GPJ_OK;
+}
+
+int gpj_ctx_destroy(gpj_ctx *ctx) {
+  if (ctx == nullptr) return GPJ_OK;
+  cudaSetDevice(ctx->device);
+  cudaFree(ctx->scratch);
+  cudaFree(ctx->staging);
+  cudaFree(ctx->host_index);
+  cudaFree(ctx->host_results);
+  cudaFreeHost(ctx->pinned);
+  delete ctx;
+  return GPJ_OK;
+}
+
+int gpj_compile(const char *query, uint64_t wildcard_limit, uint8_t *h_ir,
+                uint64_t ir_capacity, uint64_t *ir_len, uint64_t *max_depth,
+                uint64_t *num_result_slots) {
+  if (query == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null query");
+  try {
+    const gpjb::CompiledIr c = gpjb::compile_query(query, wildcard_limit);
+    if (ir_len) *ir_len = c.ir.size();
+    if (max_depth) *max_depth = c.max_depth;
+    if (num_result_slots) *num_result_slots = c.num_result_slots;
+    if (c.ir.size() > ir_capacity || (h_ir == nullptr && !c.ir.empty()))
+      return fail(GPJ_ERR_CAPACITY, "IR buffer too small: need " + std::to_string(c.ir.size()));
+    std::memcpy(h_ir, c.ir.data(), c.ir.size());
+    return GPJ_OK;
+  } catch (const gpjb::CompileError &e) {
+    return fail(e.code, e.message);
+  } catch (const std::exception &e) {
+    return fail(GPJ_ERR_IMPLEMENTATION, e.what());
+  }
+}
+
+int gpj_index_build(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_bytes,
+                    int num_levels, uint32_t flags, gpj_index *out, void *stream_) {
+  if (out == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null output");
+  std::memset(out, 0, sizeof(*out));
+  int rc = check_levels(num_levels);
+  if (rc == GPJ_OK) rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  if (size_bytes > 0 && d_input == nullptr)
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "null input with nonzero size");
+  auto stream = static_cast<cudaStream_t>(stream_);
+  const bool eq = (flags & GPJ_INDEX_EMIT_ESCAPE_QUOTE) != 0;
+  uint64_t cap = nl_capacity_guess(size_bytes);
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    rc = alloc_index(out, size_bytes, num_levels, eq, cap);
+    if (rc != GPJ_OK) return rc;
+    out->d_input = d_input;
+    out->size_bytes = size_bytes;
+    rc = enqueue_index(ctx, d_input, size_bytes, num_levels, flags, *out, stream);
+    uint64_t lines = 0;
+    int in_string = 0, depth = -1;
+    if (rc == GPJ_OK) rc = read_summary(ctx, size_bytes, stream, &lines, &in_string, &depth);
+    if (rc != GPJ_OK) {
+      release_index(out);
+      return rc;
+    }
+    out->num_lines = lines;
+    out->final_in_string = in_string;
+    out->final_depth = depth;
+    if (lines <= cap) return GPJ_OK;
+    release_index(out);
+    cap = lines;  // exact size, second pass
+  }
+  return fail(GPJ_ERR_IMPLEMENTATION, "newline capacity retry failed");
+}
+
+int gpj_index_build_async(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_bytes,
+                          int num_levels, uint32_t flags, gpj_index *index,
+                          uint64_t *d_summary, void *stream_) {
+  if (index == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null index");
+  int rc = check_levels(num_levels);
+  if (rc == GPJ_OK) rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  const uint64_t W = (size_bytes + 63u) / 64u;
+  if (W > 0 && (index->d_string == nullptr || (num_levels > 0 && index->d_leveled == nullptr)))
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "missing output buffers");
+  if ((flags & GPJ_INDEX_EMIT_ESCAPE_QUOTE) && W > 0 &&
+      (index->d_escape == nullptr || index->d_quote == nullptr))
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "escape/quote buffers required");
+  auto stream = static_cast<cudaStream_t>(stream_);
+  index->d_input = d_input;
+  index->size_bytes = size_bytes;
+  index->num_words = W;
+  index->num_levels = num_levels;
+  rc = enqueue_index(ctx, d_input, size_bytes, num_levels, flags, *index, stream);
+  if (rc != GPJ_OK) return rc;
+  if (d_summary != nullptr) {
+    GPJ_CUDA(cudaMemcpyAsync(d_summary, summary_ptr(ctx, size_bytes), 24,
+                             cudaMemcpyDeviceToDevice, stream),
+             "copy summary");
+    GPJ_CUDA(cudaMemsetAsync(d_summary + 3, 0, 8, stream), "cudaMemsetAsync");
+    if (size_bytes > 0)
+      GPJ_CUDA(cudaMemcpyAsync(d_summary + 3, error_ptr(ctx, size_bytes), 4,
+                               cudaMemcpyDeviceToDevice, stream),
+               "copy error word");
+  }
+  return GPJ_OK;
+}
+
+int gpj_index_free(gpj_ctx *ctx, gpj_index *index) {
+  (void)ctx;
+  if (index != nullptr) release_index(index);
+  return GPJ_OK;
+}
+
+int gpj_query_run(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
+                  uint64_t ir_len, uint32_t num_result_slots, int32_t *d_out, void *stream) {
+  return run_query<int32_t>(ctx, index, h_ir, ir_len, num_result_slots, d_out,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int gpj_query_run64(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
+                    uint64_t ir_len, uint32_t num_result_slots, int64_t *d_out, void *stream) {
+  return run_query<int64_t>(ctx, index, h_ir, ir_len, num_result_slots, d_out,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int gpj_query_run_opts(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
+                       uint64_t ir_len, uint32_t num_result_slots, const gpj_query_opts *opts,
+                       void *d_out, void *stream) {
+  const uint32_t base = opts ? opts->base_level : 0u;
+  const uint32_t width = opts && opts->offset_bytes ? opts->offset_bytes : 4u;
+  if (width == 8)
+    return run_query<int64_t>(ctx, index, h_ir, ir_len, num_result_slots,
+                              static_cast<int64_t *>(d_out), static_cast<cudaStream_t>(stream),
+                              base);
+  if (width != 4) return fail(GPJ_ERR_INVALID_ARGUMENT, "offset_bytes must be 4 or 8");
+  return run_query<int32_t>(ctx, index, h_ir, ir_len, num_result_slots,
+                            static_cast<int32_t *>(d_out), static_cast<cudaStream_t>(stream),
+                            base);
+}
+
+int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes, int num_levels,
+                   uint32_t num_queries, const uint8_t *const *h_irs, const uint64_t *ir_lens,
+                   const uint32_t *num_result_slots, const uint32_t *base_levels,
+                   int32_t *const *h_out, const uint64_t *out_capacity, uint64_t *num_lines,
+                   void *stream_) {
+  int rc = check_levels(num_levels);
+  if (rc == GPJ_OK) rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  if (size_bytes > 0 && h_input == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null input");
+  if (num_queries > 0 && (h_irs == nullptr || ir_lens == nullptr || num_result_slots == nullptr ||
+                          h_out == nullptr || out_capacity == nullptr))
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "null query arrays");
+  auto stream = static_cast<cudaStream_t>(stream_);
+  const uint64_t n = size_bytes;
+  const uint64_t W = (n + 63u) / 64u;
+  // one device region: input | S | LB | NL
+  const uint64_t in_bytes = round256(n);
+  const uint64_t s_bytes = round256(W * 8u);
+  const uint64_t lb_bytes = round256(W * 8u * uint64_t(num_levels));
+  uint64_t cap = nl_capacity_guess(n);
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const uint64_t nl_bytes = round256(cap * 8u);
+    rc = ensure(ctx->host_index, ctx->host_index_bytes, in_bytes + s_bytes + lb_bytes + nl_bytes);
+    if (rc != GPJ_OK) return rc;
+    auto *base = static_cast<unsigned char *>(ctx->host_index);
+    gpj_index ix;
+    std::memset(&ix, 0, sizeof(ix));
+    auto *d_in = reinterpret_cast<uint8_t *>(base);
+    ix.d_input = d_in;
+    ix.size_bytes = n;
+    ix.d_string = reinterpret_cast<uint64_t *>(base + in_bytes);
+    ix.d_leveled = reinterpret_cast<uint64_t *>(base + in_bytes + s_bytes);
+    ix.d_newline = reinterpret_cast<int64_t *>(base + in_bytes + s_bytes + lb_bytes);
+    ix.newline_capacity = cap;
+    ix.num_words = W;
+    ix.num_levels = num_levels;
+    if (n > 0)
+      GPJ_CUDA(cudaMemcpyAsync(d_in, h_input, n, cudaMemcpyHostToDevice, stream), "copy input");
+    rc = enqueue_index(ctx, d_in, n, num_levels, 0u, ix, stream);
+    uint64_t lines = 0;
+    int in_string = 0, depth = -1;
+    if (rc == GPJ_OK) rc = read_summary(ctx, n, stream, &lines, &in_string, &depth);
+    if (rc != GPJ_OK) return rc;
+    if (n == 0) {
+      if (num_lines) *num_lines = 0;  // the reference executes nothing for an empty partition
+      return GPJ_OK;
+    }
+    if (num_lines) *num_lines = lines;
+    if (lines > cap) {
+      cap = lines;
+      continue;
+    }
+    ix.num_lines = lines;
+    // results: one device region, one slice per query
+    uint64_t total = 0;
+    for (uint32_t q = 0; q < num_queries; ++q) {
+      const uint64_t need = lines * uint64_t(num_result_slots[q]) * 2u;
+      if (need > out_capacity[q])
+        return fail(GPJ_ERR_CAPACITY, "result buffer of query " + std::to_string(q) +
+                                          " needs " + std::to_string(need) + " int32");
+      total += round256(need * 4u);
+    }
+    rc = ensure(ctx->host_results, ctx->host_results_bytes, total);
+    if (rc != GPJ_OK) return rc;
+    uint64_t off = 0;
+    for (uint32_t q = 0; q < num_queries; ++q) {
+      auto *d_out = reinterpret_cast<int32_t *>(static_cast<unsigned char *>(ctx->host_results) + off);
+      rc = run_query<int32_t>(ctx, &ix, h_irs[q], ir_lens[q], num_result_slots[q], d_out, stream,
+                              base_levels ? base_levels[q] : 0u);
+      if (rc != GPJ_OK) return rc;
+      const uint64_t need = lines * uint64_t(num_result_slots[q]) * 2u;
+      if (need > 0)
+        GPJ_CUDA(cudaMemcpyAsync(h_out[q], d_out, need * 4u, cudaMemcpyDeviceToHost, stream),
+                 "copy results");
+      off += round256(need * 4u);
+    }
+    GPJ_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    return GPJ_OK;
+  }
+  return fail(GPJ_ERR_IMPLEMENTATION, "newline capacity retry failed");
+}
+
+}  // extern "C"

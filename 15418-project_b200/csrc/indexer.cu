@@ -1,0 +1,564 @@
+// Fused single-pass structural indexer for sm_100a.
+//
+// One launch replaces the reference's whole SharememIndexBuilder chain
+// (src/gpjson/index/sharemem_index_builder.cu:443-458: nine kernels, three
+// thrust scans, four scalar copies, seven passes over the input).  Each CTA
+// takes one 32 KiB tile in ticket order, stages it in shared memory with one
+// TMA tensor load (128-byte swizzle so that every thread reads its own
+// 128-byte row with conflict-free 16-byte loads), and computes per 64-byte
+// word:
+//   escape bitmap E   (word-local carry rule, escape-index.cu:29-96)
+//   quote bitmap  Q   = '"' & ~E                     (quote-index.cu:29-95)
+//   string mask   S   = prefix-XOR of Q over the file (string-index.cu:3-31)
+//   depth             = -1 + running sum of '{[' minus '}]' outside strings,
+//                       signed char                  (leveled-bitmaps-*.cu)
+//   leveled bitmaps   LB[level*W + w]
+//   newline index     NL = [0, offsets of every '\n'] (newline-*.cu)
+// The three file-wide carries (string parity, depth, newline count) cross
+// tiles through a decoupled look-back.  A tile's depth change depends on the
+// string state it starts in, so its look-back descriptor holds the change for
+// both start states; descriptors compose associatively.
+#include "bits.cuh"
+#include "indexer.cuh"
+
+#include <cudaTypedefs.h>
+
+namespace gpjb {
+namespace {
+
+// ----------------------------------------------------------------------------
+// Look-back descriptor: one 64-bit word per tile, written with one store.
+//   bits 0-1  status (0 = not ready, 1 = aggregate, 2 = inclusive prefix)
+//   bit  2    string parity of the tile (quotes it toggles, mod 2)
+//   bits 3-10 depth change if the tile starts outside a string (mod 256)
+//   bits 11-18 depth change if it starts inside a string (mod 256)
+//   bits 19-63 newline count
+// An inclusive descriptor holds the prefix from the start of the partition,
+// evaluated for the initial state (outside a string, depth -1): its bit 2 is
+// the string state after the tile and bits 3-10 the depth sum.
+// ----------------------------------------------------------------------------
+constexpr uint64_t kStatusAgg = 1, kStatusIncl = 2;
+
+struct Agg {
+  uint32_t p;   // string parity
+  uint32_t d0;  // depth change starting outside a string (mod 256)
+  uint32_t d1;  // depth change starting inside a string (mod 256)
+  uint64_t n;   // newlines
+};
+
+__device__ __forceinline__ Agg agg_identity() { return Agg{0u, 0u, 0u, 0ull}; }
+
+// `a` covers the bytes before `b`.
+__device__ __forceinline__ Agg agg_combine(const Agg &a, const Agg &b) {
+  Agg r;
+  r.p = a.p ^ b.p;
+  r.d0 = (a.d0 + (a.p ? b.d1 : b.d0)) & 0xFFu;
+  r.d1 = (a.d1 + (a.p ? b.d0 : b.d1)) & 0xFFu;
+  r.n = a.n + b.n;
+  return r;
+}
+
+__device__ __forceinline__ uint64_t agg_pack(uint64_t status, const Agg &a) {
+  return status | (uint64_t(a.p & 1u) << 2) | (uint64_t(a.d0 & 0xFFu) << 3) |
+         (uint64_t(a.d1 & 0xFFu) << 11) | (a.n << 19);
+}
+
+__device__ __forceinline__ Agg agg_unpack(uint64_t v) {
+  Agg a;
+  a.p = uint32_t(v >> 2) & 1u;
+  a.d0 = uint32_t(v >> 3) & 0xFFu;
+  a.d1 = uint32_t(v >> 11) & 0xFFu;
+  a.n = v >> 19;
+  return a;
+}
+
+__device__ __forceinline__ Agg shfl_down_agg(const Agg &a, int off) {
+  Agg r;
+  r.p = __shfl_down_sync(0xFFFFFFFFu, a.p, off);
+  r.d0 = __shfl_down_sync(0xFFFFFFFFu, a.d0, off);
+  r.d1 = __shfl_down_sync(0xFFFFFFFFu, a.d1, off);
+  r.n = __shfl_down_sync(0xFFFFFFFFu, a.n, off);
+  return r;
+}
+
+__device__ __forceinline__ uint64_t ld_relaxed(const unsigned long long *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long *p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Every wait is bounded: after this many polls (with back-off) the kernel
+// records an error bit and carries on with neutral values, so a broken
+// invariant surfaces as an error status on the host instead of a hang.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Warp 0 only.  Publishes the tile's aggregate, walks back over predecessors
+// 32 at a time and returns the exclusive prefix of the tile.
+__device__ Agg lookback(const IndexLaunch &P, uint32_t tile, const Agg &local) {
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) return agg_identity();
+  if (lane == 0) st_relaxed(&P.tile_state[tile], agg_pack(kStatusAgg, local));
+
+  Agg later = agg_identity();
+  int64_t base = int64_t(tile) - 1;
+  for (;;) {
+    const int64_t idx = base - lane;
+    uint64_t s = 0;
+    uint32_t polls = 0;
+    for (;;) {
+      s = (idx >= 0) ? ld_relaxed(&P.tile_state[idx]) : kStatusIncl;
+      const bool ready = (s & 3u) != 0;
+      if (__all_sync(0xFFFFFFFFu, ready)) break;
+      if (++polls > kSpinLimit) {
+        if (lane == 0) atomicOr(P.error, kErrLookbackTimeout);
+        if (!ready) s = kStatusIncl;
+        break;
+      }
+      __nanosleep(polls < 64 ? 20 : 500);
+    }
+    const uint32_t incl = __ballot_sync(0xFFFFFFFFu, (s & 3u) == kStatusIncl);
+    const int limit = incl ? (__ffs(incl) - 1) : 31;
+    Agg v = (lane <= limit) ? agg_unpack(s) : agg_identity();
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const Agg o = shfl_down_agg(v, off);  // tiles further back
+      if (lane + off < 32) v = agg_combine(o, v);
+    }
+    Agg window;
+    window.p = __shfl_sync(0xFFFFFFFFu, v.p, 0);
+    window.d0 = __shfl_sync(0xFFFFFFFFu, v.d0, 0);
+    window.d1 = __shfl_sync(0xFFFFFFFFu, v.d1, 0);
+    window.n = __shfl_sync(0xFFFFFFFFu, v.n, 0);
+    later = agg_combine(window, later);
+    if (incl) break;
+    base -= 32;
+  }
+  return later;
+}
+
+// ----------------------------------------------------------------------------
+// Leveled bitmaps of one word.  Walks the open/close events of the word in
+// order; separators between two events share one depth.  Depth arithmetic is
+// signed char, as in sharemem/leveled-bitmaps-index.cu:270-300.
+// ----------------------------------------------------------------------------
+template <int LMAX>
+__device__ __forceinline__ void add_level(uint64_t (&lb)[LMAX], int d,
+                                          uint64_t m, int L) {
+  if (m == 0 || d < 0 || d >= L) return;
+#pragma unroll
+  for (int l = 0; l < LMAX; ++l)
+    if (d == l) lb[l] |= m;
+}
+
+template <int LMAX>
+__device__ __forceinline__ int leveled_word(uint64_t op, uint64_t cl,
+                                            uint64_t sp, int depth, int L,
+                                            uint64_t (&lb)[LMAX]) {
+#pragma unroll
+  for (int l = 0; l < LMAX; ++l) lb[l] = 0;
+  uint64_t ev = op | cl;
+  if (ev == 0) {
+    add_level<LMAX>(lb, depth, sp, L);
+    return depth;
+  }
+  int d = depth;
+  uint64_t acc = 0, done = 0;
+  while (ev) {
+    const uint64_t bit = ev & (0 - ev);
+    const uint64_t below = bit - 1;
+    acc |= sp & below & ~done;
+    if (op & bit) {
+      add_level<LMAX>(lb, d, acc, L);
+      d = int(int8_t(d + 1));
+      acc = bit;
+    } else {
+      add_level<LMAX>(lb, d, acc | bit, L);
+      d = int(int8_t(d - 1));
+      acc = 0;
+    }
+    done = below | bit;
+    ev &= ev - 1;
+  }
+  add_level<LMAX>(lb, d, acc | (sp & ~done), L);
+  return d;
+}
+
+__device__ __forceinline__ uint64_t valid_mask(uint64_t w, uint64_t n) {
+  const uint64_t base = w * 64u;
+  if (base + 64u <= n) return ~0ull;
+  if (base >= n) return 0ull;
+  return (1ull << (n - base)) - 1ull;
+}
+
+__device__ __forceinline__ void store2(uint64_t *dst, uint64_t w, uint64_t W,
+                                       uint64_t a, uint64_t b) {
+  // dst + w is 16-byte aligned whenever the element offset is even
+  if (w + 1 < W) {
+    if (((reinterpret_cast<uintptr_t>(dst + w)) & 15u) == 0) {
+      *reinterpret_cast<ulonglong2 *>(dst + w) = make_ulonglong2(a, b);
+    } else {
+      dst[w] = a;
+      dst[w + 1] = b;
+    }
+  } else if (w < W) {
+    dst[w] = a;
+  }
+}
+
+// Loads 64 bytes [base, base+64) of the input as 16 registers, zero past n.
+__device__ __forceinline__ void load_word_global(const uint8_t *in, uint64_t n,
+                                                 uint64_t base, uint32_t (&r)[16]) {
+  if (base + 64u <= n && (reinterpret_cast<uintptr_t>(in + base) & 15u) == 0) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(in + base);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const uint4 v = __ldg(p + c);
+      r[4 * c + 0] = v.x;
+      r[4 * c + 1] = v.y;
+      r[4 * c + 2] = v.z;
+      r[4 * c + 3] = v.w;
+    }
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const uint64_t i = base + uint64_t(4 * k + b);
+      if (i < n) v |= uint32_t(in[i]) << (8 * b);
+    }
+    r[k] = v;
+  }
+}
+
+// Reads word `half` (0 or 1) of row `row` from the swizzled tile: chunk j of
+// a row sits at chunk position j ^ (row & 7) (TMA 128-byte swizzle).
+__device__ __forceinline__ void load_word_smem(const uint8_t *tile, int row,
+                                               int half, uint32_t (&r)[16]) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int j = 4 * half + c;
+    const uint4 v = *reinterpret_cast<const uint4 *>(
+        tile + row * 128 + ((j ^ (row & 7)) << 4));
+    r[4 * c + 0] = v.x;
+    r[4 * c + 1] = v.y;
+    r[4 * c + 2] = v.z;
+    r[4 * c + 3] = v.w;
+  }
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+template <int LMAX, bool kTma>
+__global__ void __launch_bounds__(kIndexThreads)
+    index_kernel(const __grid_constant__ CUtensorMap tmap, const IndexLaunch P) {
+  __shared__ __align__(1024) uint8_t s_tile[kTma ? kTileBytes : 16];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ uint32_t s_tile_id;
+  __shared__ uint32_t s_halo;
+  __shared__ uint32_t s_last_tp[8];
+  __shared__ uint32_t s_warp_par[8];
+  __shared__ uint32_t s_warp_dd[8];
+  __shared__ uint32_t s_warp_nl[8];
+  __shared__ uint32_t s_prefix_p, s_prefix_d;
+  __shared__ unsigned long long s_prefix_n;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+
+  if (tid == 0) s_tile_id = atomicAdd(P.tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile_id;
+  if (tile >= P.num_tiles) return;  // cannot happen with grid == num_tiles
+  const uint64_t tile_byte0 = uint64_t(tile) * kTileBytes;
+  const uint64_t tile_word0 = uint64_t(tile) * kTileWords;
+  const int64_t row0 = int64_t(tile) * kTileRows;
+
+  if constexpr (kTma) {
+    if (tid == 0) {
+      const uint32_t bar = smem_u32(&s_bar);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile(
+          "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+          "r"(uint32_t(kTileBytes))
+          : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(s_tile)),
+          "l"(&tmap), "r"(0), "r"(int32_t(row0)), "r"(bar)
+          : "memory");
+    }
+  }
+  // Escape carry into the tile: parity of the backslash run that ends the
+  // previous word (read backward, at most 64 bytes).
+  if (tid == 0) {
+    uint32_t p = 0;
+    if (tile > 0) {
+      for (int k = 1; k <= 64; ++k) {
+        if (P.in[tile_byte0 - uint64_t(k)] == '\\') p ^= 1u;
+        else break;
+      }
+    }
+    s_halo = p;
+  }
+
+  const int64_t my_row = row0 + tid;
+  const uint64_t w0 = tile_word0 + 2u * uint64_t(tid);  // my first word
+  uint32_t r[16];
+  WordClasses c0, c1;
+  if constexpr (kTma) {
+    if (my_row >= int64_t(P.full_rows)) {
+      load_word_global(P.in, P.n, w0 * 64u, r);
+      c0 = classify64(r);
+      load_word_global(P.in, P.n, w0 * 64u + 64u, r);
+      c1 = classify64(r);
+      // still take part in the barrier wait below via the shared path
+    }
+    {
+      const uint32_t bar = smem_u32(&s_bar);
+      uint32_t done = 0, polls = 0;
+      while (!done) {
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;"
+            " selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+        if (!done && ++polls > kSpinLimit) {
+          atomicOr(P.error, kErrTmaTimeout);
+          break;
+        }
+      }
+    }
+    if (my_row < int64_t(P.full_rows)) {
+      load_word_smem(s_tile, tid, 0, r);
+      c0 = classify64(r);
+      load_word_smem(s_tile, tid, 1, r);
+      c1 = classify64(r);
+    }
+  } else {
+    load_word_global(P.in, P.n, w0 * 64u, r);
+    c0 = classify64(r);
+    load_word_global(P.in, P.n, w0 * 64u + 64u, r);
+    c1 = classify64(r);
+  }
+
+  // --- escape carries between words --------------------------------------
+  const uint32_t tp0 = trailing_escape_parity(c0.bs);
+  const uint32_t tp1 = trailing_escape_parity(c1.bs);
+  if (lane == 31) s_last_tp[warp] = tp1;
+  __syncthreads();  // (1) s_last_tp, s_halo
+  uint32_t cin0 = __shfl_up_sync(0xFFFFFFFFu, tp1, 1);
+  if (lane == 0) cin0 = (warp == 0) ? s_halo : s_last_tp[warp - 1];
+
+  const uint64_t E0 = escaped_bits(c0.bs, cin0);
+  const uint64_t E1 = escaped_bits(c1.bs, tp0);
+  const uint64_t Q0 = c0.qt & ~E0;
+  const uint64_t Q1 = c1.qt & ~E1;
+  const uint64_t Sl0 = prefix_xor(Q0);
+  const uint64_t Sl1 = prefix_xor(Q1);
+  const uint32_t par0 = uint32_t(popc64(Q0)) & 1u;
+  const uint32_t par1 = uint32_t(popc64(Q1)) & 1u;
+
+  // depth change of each word if it starts outside a string, and in total
+  const int d00 = popc64(c0.op & ~Sl0) - popc64(c0.cl & ~Sl0);
+  const int t0 = popc64(c0.op) - popc64(c0.cl);
+  const int d10 = popc64(c1.op & ~Sl1) - popc64(c1.cl & ~Sl1);
+  const int t1 = popc64(c1.op) - popc64(c1.cl);
+  const int thr_d0 = d00 + (par0 ? (t1 - d10) : d10);
+  const int thr_t = t0 + t1;
+  const uint32_t thr_par = par0 ^ par1;
+  const uint32_t thr_nl = uint32_t(popc64(c0.nl) + popc64(c1.nl));
+
+  // --- tile-local exclusive scans ------------------------------------------
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const uint32_t par_ballot = __ballot_sync(0xFFFFFFFFu, thr_par);
+  uint32_t pex = uint32_t(__popc(par_ballot & lt_mask)) & 1u;
+  if (lane == 0) s_warp_par[warp] = uint32_t(__popc(par_ballot)) & 1u;
+  __syncthreads();  // (2)
+  for (int w = 0; w < warp; ++w) pex ^= s_warp_par[w];
+  uint32_t tile_par = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) tile_par ^= s_warp_par[w];
+
+  // depth changes are only needed mod 256: two 16-bit lanes cannot overflow
+  // over 256 threads (256 * 255 < 65536)
+  const int dt0 = pex ? (thr_t - thr_d0) : thr_d0;
+  uint32_t dd = (uint32_t(dt0) & 0xFFu) | ((uint32_t(thr_t) & 0xFFu) << 16);
+  uint32_t nl = thr_nl;
+  uint32_t dd_inc = dd, nl_inc = nl;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t a = __shfl_up_sync(0xFFFFFFFFu, dd_inc, off);
+    const uint32_t b = __shfl_up_sync(0xFFFFFFFFu, nl_inc, off);
+    if (lane >= off) {
+      dd_inc += a;
+      nl_inc += b;
+    }
+  }
+  if (lane == 31) {
+    s_warp_dd[warp] = dd_inc;
+    s_warp_nl[warp] = nl_inc;
+  }
+  __syncthreads();  // (3)
+  uint32_t dd_ex = dd_inc - dd, nl_ex = nl_inc - nl;
+  uint32_t tile_dd = 0, tile_nl = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    if (w < warp) {
+      dd_ex += s_warp_dd[w];
+      nl_ex += s_warp_nl[w];
+    }
+    tile_dd += s_warp_dd[w];
+    tile_nl += s_warp_nl[w];
+  }
+
+  // --- decoupled look-back --------------------------------------------------
+  if (warp == 0) {
+    Agg local;
+    local.p = tile_par;
+    local.d0 = tile_dd & 0xFFu;
+    local.d1 = ((tile_dd >> 16) - tile_dd) & 0xFFu;  // total - d0
+    local.n = tile_nl;
+    const Agg prefix = lookback(P, tile, local);
+    if (lane == 0) {
+      const Agg incl = agg_combine(prefix, local);
+      st_relaxed(&P.tile_state[tile], agg_pack(kStatusIncl, incl));
+      s_prefix_p = prefix.p;
+      s_prefix_d = prefix.d0;
+      s_prefix_n = prefix.n;
+      if (tile + 1 == P.num_tiles) {
+        P.summary[0] = incl.n + 1u;  // lines = newlines + 1
+        P.summary[1] = incl.p;
+        P.summary[2] = uint64_t(int64_t(int8_t(uint8_t(incl.d0 - 1u))));
+      }
+      if (tile == 0 && P.nl_cap > 0) P.NL[0] = 0;
+    }
+  }
+  __syncthreads();  // (4)
+  const uint32_t c_in = s_prefix_p;
+  const uint32_t d_in = s_prefix_d;
+  const uint64_t nl_base = s_prefix_n + nl_ex;
+
+  // --- outputs ----------------------------------------------------------------
+  const uint32_t car0 = c_in ^ pex;
+  const uint32_t car1 = car0 ^ par0;
+  const uint64_t S0 = Sl0 ^ (car0 ? ~0ull : 0ull);
+  const uint64_t S1 = Sl1 ^ (car1 ? ~0ull : 0ull);
+  const uint32_t a_ex = dd_ex & 0xFFu, t_ex = (dd_ex >> 16) & 0xFFu;
+  const int depth0 = int(int8_t(uint8_t(d_in - 1u + (c_in ? (t_ex - a_ex) : a_ex))));
+
+  store2(P.S, w0, P.W, S0, S1);
+  if (P.E != nullptr) {
+    store2(P.E, w0, P.W, E0 & valid_mask(w0, P.n), E1 & valid_mask(w0 + 1, P.n));
+    store2(P.Q, w0, P.W, Q0, Q1);
+  }
+
+  if (P.num_levels > 0) {
+    uint64_t lb0[LMAX], lb1[LMAX];
+    const int depth1 = leveled_word<LMAX>(c0.op & ~S0, c0.cl & ~S0, c0.sp & ~S0,
+                                          depth0, P.num_levels, lb0);
+    leveled_word<LMAX>(c1.op & ~S1, c1.cl & ~S1, c1.sp & ~S1, depth1,
+                       P.num_levels, lb1);
+#pragma unroll
+    for (int l = 0; l < LMAX; ++l) {
+      if (l < P.num_levels) store2(P.LB + uint64_t(l) * P.W, w0, P.W, lb0[l], lb1[l]);
+    }
+  }
+
+  // newline offsets (every '\n' counts, strings or not)
+  uint64_t k = nl_base;
+  uint64_t m = c0.nl;
+  while (m) {
+    const int b = __ffsll(static_cast<long long>(m)) - 1;
+    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t(w0 * 64u + uint64_t(b));
+    ++k;
+    m &= m - 1;
+  }
+  m = c1.nl;
+  while (m) {
+    const int b = __ffsll(static_cast<long long>(m)) - 1;
+    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t((w0 + 1) * 64u + uint64_t(b));
+    ++k;
+    m &= m - 1;
+  }
+}
+
+template <int LMAX>
+cudaError_t launch_levels(const IndexLaunch &L, const CUtensorMap *map,
+                          bool use_tma, cudaStream_t stream) {
+  const dim3 grid(L.num_tiles), block(kIndexThreads);
+  if (use_tma) {
+    index_kernel<LMAX, true><<<grid, block, 0, stream>>>(*map, L);
+  } else {
+    CUtensorMap dummy{};
+    index_kernel<LMAX, false><<<grid, block, 0, stream>>>(dummy, L);
+  }
+  return cudaGetLastError();
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
+                                &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      p = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+}  // namespace
+
+void index_bind_scratch(IndexLaunch &L, void *scratch) {
+  auto *base = static_cast<unsigned char *>(scratch);
+  L.tile_state = reinterpret_cast<unsigned long long *>(base);
+  unsigned char *tail = base + uint64_t(L.num_tiles) * 8u;
+  L.summary = reinterpret_cast<unsigned long long *>(tail);        // 4 x u64
+  L.tile_counter = reinterpret_cast<unsigned int *>(tail + 32);
+  L.error = reinterpret_cast<unsigned int *>(tail + 36);
+}
+
+bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n) {
+  const uint64_t rows = n / 128u;
+  if (rows == 0 || (reinterpret_cast<uintptr_t>(in) & 15u) != 0) return false;
+  auto fn = encode_fn();
+  if (fn == nullptr) return false;
+  const cuuint64_t dims[2] = {128u, rows};
+  const cuuint64_t strides[1] = {128u};
+  const cuuint32_t box[2] = {128u, uint32_t(kTileRows)};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                        const_cast<uint8_t *>(in), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+cudaError_t index_launch(const IndexLaunch &L, const CUtensorMap *map,
+                         bool use_tma, cudaStream_t stream) {
+  if (L.num_tiles == 0) return cudaSuccess;
+  const uint64_t scratch = uint64_t(L.num_tiles) * 8u + 64u;
+  cudaError_t e = cudaMemsetAsync(L.tile_state, 0, scratch, stream);
+  if (e != cudaSuccess) return e;
+  const int lv = L.num_levels;
+  if (lv <= 2) return launch_levels<2>(L, map, use_tma, stream);
+  if (lv <= 4) return launch_levels<4>(L, map, use_tma, stream);
+  if (lv <= 8) return launch_levels<8>(L, map, use_tma, stream);
+  return launch_levels<kMaxLevels>(L, map, use_tma, stream);
+}
+
+}  // namespace gpjb

@@ -1,0 +1,39 @@
+// Host-side interface of the JSONPath query kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace gpjb {
+
+constexpr int kMaxQueryLevels = 16;   // orig.hpp:10 kMaxQueryLevels
+constexpr int kMaxQueryIrBytes = 4096;  // orig.hpp:11 kMaxQueryIrBytes
+
+// One query over every record of one partition.
+struct QueryLaunch {
+  const uint8_t *in = nullptr;   // partition bytes
+  int64_t n = 0;
+  const int64_t *NL = nullptr;   // newline index
+  int64_t num_lines = 0;
+  const uint64_t *S = nullptr;   // string mask [W]
+  const uint64_t *LB = nullptr;  // leveled bitmaps [L*W]
+  int64_t W = 0;
+  int ir_len = 0;
+  int num_results = 0;           // result slots per record
+  int num_levels = 0;            // levels present in LB; deeper reads see 0
+  int base_level = 0;            // bitmap level of query level 0 (1: elements
+                                 // of a top-level array are the records)
+  int32_t *out32 = nullptr;      // [num_lines][num_results][2], or
+  int64_t *out64 = nullptr;      // the same with 64-bit offsets
+};
+
+// The IR travels in the kernel parameters (4 KiB, copied into shared memory
+// by every CTA), so concurrent launches never share an IR buffer.
+struct IrBlob {
+  uint8_t bytes[kMaxQueryIrBytes];
+};
+
+cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
+                         int block, cudaStream_t stream);
+
+}  // namespace gpjb

@@ -1,0 +1,404 @@
+"""Benchmark: GpJSON index + query throughput on B200 (one JSON line on stdout).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1|c0|c2]
+
+A step is one pass of the hot path over the workload: the fused structural
+index build of the whole input plus every query of the workload, with the
+input already resident in device memory.  `value` is input GB (1e9 B) per
+second over all ranks; `e2e` is the same metric through the public C ABI
+call that takes host buffers (gpj_query_host: H2D of the input, index, all
+queries, D2H of every result array) from pinned memory.
+
+Workloads (seeded synthetic stand-ins for the GpJSON datasets):
+  c1  one 1 GiB top-level array of ~2 KiB product records, one element per
+      line; query $[*].categoryPath[1:3].id   (default)
+  c0  64 MiB NDJSON of ~2 KiB post records; query $.user.lang
+  c2  4 GiB NDJSON post records (deeper nesting); four queries over one index
+
+Multi-GPU (--gpus N under torchrun): the path has no exchange step, so each
+rank runs an independent replica of the workload ("scaling": "weak") and the
+timed region is the max over ranks.
+
+--impl reference times the reference algorithm's CPU restatement (the
+oracle: the reference project has no CPU implementation of this path) on the
+host cores, on a bounded sample of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__ as entry  # noqa: E402
+
+METRIC = "index+query GB/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def workload(name: str, pkg):
+    dg = pkg.datagen
+    if name == "c0":
+        data = dg.tweets(0, 64 << 20)
+        queries, records = ["$.user.lang"], "lines"
+        desc = "c0: 64 MiB NDJSON post records (~2 KiB, depth<=6), $.user.lang"
+    elif name == "c1":
+        data = dg.products(1, 1 << 30)
+        queries, records = ["$[*].categoryPath[1:3].id"], "array"
+        desc = ("c1: 1 GiB single top-level array of ~2 KiB product records, "
+                "$[*].categoryPath[1:3].id")
+    elif name == "c2":
+        data = dg.tweets(2, 4 << 30, deep=True)
+        queries = ["$.user.lang", "$.entities.hashtags[*].text", "$.place.country_code",
+                   "$.retweeted_status.user.id"]
+        records = "lines"
+        desc = "c2: 4 GiB NDJSON post records (depth<=8), 4 queries over one index"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return data, queries, records, desc
+
+
+def compile_all(pkg, queries):
+    """Compiles the workload queries; "$[*]..." selects array elements as records
+    (bitmap level offset 1) and "[*]" inside a path expands to [0:8]."""
+    out = []
+    for q in queries:
+        base = 0
+        text = q
+        if q.startswith("$[*]"):
+            base, text = 1, "$" + q[4:]
+        out.append((pkg.compile(text, wildcard_limit=8), base))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def dist_init():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def algorithmic_index_bytes(n: int, levels: int, lines: int) -> int:
+    # input read once + S + L leveled words + newline index (int64)
+    W = (n + 63) // 64
+    return n + 8 * W * (1 + levels) + 8 * lines
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    pkg = entry.package()
+    pkg.load_library()
+    data, queries, records, desc = workload(args.workload, pkg)
+    comp = compile_all(pkg, queries)
+    levels = max(c.max_depth + base for c, base in comp)
+    n = int(data.size)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = pkg.Context(local)
+    d_in = torch.from_numpy(data).to(dev)
+    W = (n + 63) // 64
+    S = torch.empty(W, dtype=torch.int64, device=dev)
+    LB = torch.empty(W * levels, dtype=torch.int64, device=dev)
+    nl_cap = n // 32 + 1024
+    NL = torch.empty(nl_cap, dtype=torch.int64, device=dev)
+    summ = torch.zeros(4, dtype=torch.int64, device=dev)
+    ix = pkg.Index()
+    ix.d_string, ix.d_leveled = S.data_ptr(), LB.data_ptr()
+    ix.d_newline, ix.newline_capacity = NL.data_ptr(), nl_cap
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev) if n < 2 * L2_BYTES \
+        else None
+    s = stream.cuda_stream
+
+    # one build to learn the record count and size the result buffers
+    with torch.cuda.stream(stream):
+        ctx.build_index_async(d_in.data_ptr(), n, levels, ix, summ.data_ptr(), stream=s)
+    stream.synchronize()
+    lines = int(summ[0].item())
+    assert lines <= nl_cap and int(summ[3].item()) == 0
+    ix.num_lines = lines
+    outs = [torch.empty(lines * c.num_result_slots * 2, dtype=torch.int32, device=dev)
+            for c, _ in comp]
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        ctx.build_index_async(d_in.data_ptr(), n, levels, ix, summ.data_ptr(), stream=s)
+        if ev is not None:
+            ev[1].record(stream)
+        for (c, base), o in zip(comp, outs):
+            ctx.query(ix, c, o.data_ptr(), stream=s, base_level=base)
+        if ev is not None:
+            ev[2].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    stream.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    t_index = t_total = 0.0
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            if flush is not None:
+                flush.fill_(k)
+            step(evs[k])
+    torch.cuda.synchronize(dev)
+    for e in evs:
+        t_index += e[0].elapsed_time(e[1])
+        t_total += e[0].elapsed_time(e[2])
+    barrier(world)
+    clk = clocks.stop()
+    ms_step = allreduce_max(t_total / args.steps, world)
+    ms_index = allreduce_max(t_index / args.steps, world)
+
+    # end to end through the host-buffer C ABI call
+    h_in = torch.from_numpy(data).pin_memory()
+    h_outs = [torch.empty(o.numel(), dtype=torch.int32).pin_memory() for o in outs]
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        got = ctx.query_host(h_in.data_ptr(), n, levels, [c for c, _ in comp],
+                             [h.data_ptr() for h in h_outs], [h.numel() for h in h_outs],
+                             stream=s, base_levels=[b for _, b in comp])
+        e1.record(stream)
+        e1.synchronize()
+        assert got == lines
+        if k >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
+    # bit-exact check of the e2e results against the device-resident run
+    for h, o in zip(h_outs, outs):
+        assert torch.equal(h, o.cpu()), "e2e results differ from the device-resident run"
+
+    gb = n * world / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    b_index = algorithmic_index_bytes(n, levels, lines)
+    achieved = b_index / (ms_index / 1e3) / 1e9
+    traffic_path = ROOT / "profiles" / f"traffic_{args.workload}.json"
+    traffic = None
+    if traffic_path.exists():
+        try:
+            traffic = json.loads(traffic_path.read_text()).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": round(gb / (ms_step / 1e3), 3), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": {"workload": desc, "input_bytes": n, "records": lines, "levels": levels,
+                   "queries": queries, "record_kind": records,
+                   "l2": "flushed between steps" if flush is not None else
+                         "input larger than L2", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": round(gb / (e2e_step / 1e3), 3), "unit": "GB/s",
+                "h2d_bytes_per_step": n,
+                "d2h_bytes_per_step": sum(h.numel() * 4 for h in h_outs)},
+        "gpu_launches": 1 + len(comp),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "kernel": "gpjb::index_kernel", "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": b_index,
+                     "ms_per_launch": round(ms_index, 4)},
+        "index_ms": round(ms_index, 4), "query_ms": round(ms_step - ms_index, 4),
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(data, comp, records, levels, budget_s=12.0)
+    ctx.close()
+    return line
+
+
+def _partitions(data: np.ndarray, parts: int):
+    """Newline-aligned partitions (the reference's independent partitions,
+    src/gpjson/file/file_reader.cpp:41-77)."""
+    n = data.size
+    bounds = [0]
+    for k in range(1, parts):
+        t = k * n // parts
+        nl = np.flatnonzero(data[t:min(n, t + (1 << 20))] == 10)
+        if nl.size:
+            bounds.append(t + int(nl[0]) + 1)
+    bounds.append(n)
+    bounds = sorted(set(bounds))
+    return [(a, b) for a, b in zip(bounds, bounds[1:]) if b > a]
+
+
+def cpu_baseline(data, comp, records, levels, budget_s: float, threads: int | None = None):
+    """Times the oracle (the reference algorithm restated in C) on a bounded,
+    newline-aligned sample with one partition per host thread."""
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    sample = min(data.size, 96 << 20)
+    parts = _partitions(data[:sample], threads * 4)
+
+    def work(ab):
+        a, b = ab
+        ix = oracle.OracleIndex(data[a:b], levels)
+        for c, _base in comp:
+            if _base == 0:
+                ix.query(c.ir_bytes, c.num_result_slots)
+        return b - a
+
+    t0 = time.perf_counter()
+    done = 0
+    with cf.ThreadPoolExecutor(threads) as pool:
+        for got in pool.map(work, parts):
+            done += got
+    dt = time.perf_counter() - t0
+    return {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
+            "kind": "port", "sample": f"first {done} bytes of the workload, "
+            f"{len(parts)} newline-aligned partitions, {threads} threads"}
+
+
+def run_reference(args, world, rank):
+    """CPU arm: the oracle on the host cores, same metric and config."""
+    if rank != 0:
+        return None
+    pkg = entry.package()
+    data, queries, records, desc = workload(args.workload, pkg)
+    comp = compile_all(pkg, queries)
+    levels = max(c.max_depth + base for c, base in comp)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(data, comp, records, levels, budget_s=10.0)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    cb["value"] = round(v, 4)
+    return {"metric": METRIC, "value": round(v, 4), "unit": "GB/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+            "config": {"workload": desc, "queries": queries},
+            "cpu_baseline": cb,
+            "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+    else:
+        line = run_ours(args, world, rank, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * gpjson_b200 -- C ABI of the B200 GpJSON engine.
+ *
+ * Plain pointers and sizes only.  Device pointers are marked d_, host
+ * pointers h_.  Every call returns a status (GPJ_OK = 0); the message of the
+ * last failure on the calling thread is gpj_last_error().  Streams are passed
+ * as void* (a cudaStream_t; NULL = legacy default stream).
+ *
+ * Each entry point names the reference interface it replaces
+ * (Xinyu-Li-123/15418-project, paths relative to that project).
+ */
+#ifndef GPJSON_B200_H
+#define GPJSON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The C++ wrapper maps them back onto the reference's
+ * exception types (include/gpjson/error/*.hpp, query/error.hpp, file/error.hpp,
+ * cuda/error.hpp). */
+#define GPJ_OK 0
+#define GPJ_ERR_CUDA 1              /* error::cuda::CudaError */
+#define GPJ_ERR_OOM 2               /* error::cuda::CudaError (allocation) */
+#define GPJ_ERR_MALFORMED_QUERY 3   /* error::query::MalformedQueryError */
+#define GPJ_ERR_UNSUPPORTED_QUERY 4 /* error::query::UnsupportedQueryError */
+#define GPJ_ERR_EXECUTION 5         /* error::query::QueryExecutionError */
+#define GPJ_ERR_TIMEOUT 6           /* a bounded device wait gave up */
+#define GPJ_ERR_INVALID_ARGUMENT 7  /* std::invalid_argument */
+#define GPJ_ERR_OUT_OF_RANGE 8      /* std::out_of_range */
+#define GPJ_ERR_CAPACITY 9          /* a caller buffer is too small */
+#define GPJ_ERR_IMPLEMENTATION 10   /* error::common::ImplementationError */
+
+/* gpj_index_build flags */
+#define GPJ_INDEX_EMIT_ESCAPE_QUOTE 1u /* also materialise E and Q */
+#define GPJ_INDEX_NO_TMA 2u            /* stage tiles with plain loads */
+
+#define GPJ_MAX_LEVELS 22     /* kMaxNumLevels, sharemem/leveled-bitmaps-index.cu */
+#define GPJ_MAX_QUERY_IR 4096 /* kMaxQueryIrBytes, query/kernels/orig.hpp:11 */
+#define GPJ_MAX_QUERY_DEPTH 16 /* kMaxQueryLevels, query/kernels/orig.hpp:10 */
+
+typedef struct gpj_ctx gpj_ctx;
+
+/* Built structural indexes of one partition (include/gpjson/index/index.hpp:
+ * NewlineIndex, StringIndex, LeveledBitmapIndex, BuiltIndices).  Bitmaps use
+ * the reference layout: bit b of word w <-> byte 64*w+b, leveled bitmaps
+ * level-major d_leveled[level * num_words + w]. */
+typedef struct gpj_index {
+  const uint8_t *d_input;  /* borrowed partition bytes */
+  uint64_t size_bytes;
+  int64_t *d_newline;      /* [num_lines]: 0, then every '\n' offset */
+  uint64_t num_lines;      /* newline count + 1 */
+  uint64_t newline_capacity;
+  uint64_t *d_string;      /* [num_words] in-string mask */
+  uint64_t *d_leveled;     /* [num_levels * num_words] */
+  uint64_t *d_escape;      /* [num_words] or NULL */
+  uint64_t *d_quote;       /* [num_words] or NULL */
+  uint64_t num_words;      /* ceil(size_bytes / 64) */
+  int32_t num_levels;
+  int32_t final_in_string; /* string state after the last byte */
+  int32_t final_depth;     /* signed-char depth after the last byte */
+  int32_t reserved;
+  void *owner;             /* library-owned allocation (NULL: caller-owned) */
+} gpj_index;
+
+/* Library version, major*10000 + minor*100 + patch. */
+int gpj_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *gpj_last_error(void);
+
+/* Context: device binding plus reusable device buffers.  Replaces the
+ * reference's per-call cudaMalloc/cudaFree (src/gpjson/cuda/cuda.cpp:33-47).
+ * A context may be used from one host thread at a time. */
+int gpj_ctx_create(int device, gpj_ctx **out);
+int gpj_ctx_destroy(gpj_ctx *ctx);
+
+/* Compiles a JSONPath query into the byte IR.
+ * Replaces query::QueryCompiler::compile / QueryParser::compile
+ * (include/gpjson/query/query_compiler.hpp:110-116, 86-92).  Same grammar,
+ * IR, max_depth and result-slot count.  wildcard_limit = 0 rejects "[*]" as
+ * the reference does; K > 0 compiles "[*]" as "[0:K]". */
+int gpj_compile(const char *query, uint64_t wildcard_limit, uint8_t *h_ir,
+                uint64_t ir_capacity, uint64_t *ir_len, uint64_t *max_depth,
+                uint64_t *num_result_slots);
+
+/* Builds the newline index, string mask and leveled bitmaps (and, with
+ * GPJ_INDEX_EMIT_ESCAPE_QUOTE, the escape and quote bitmaps) of one
+ * device-resident partition in one fused launch; the library allocates the
+ * outputs (free with gpj_index_free).  Returns once num_lines is known.
+ * Replaces index::IndexBuilder::build
+ * (include/gpjson/index/index_builder.hpp:55-63; builders at
+ * src/gpjson/index/{orig,fuse,sharemem}_index_builder.cu). */
+int gpj_index_build(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_bytes,
+                    int num_levels, uint32_t flags, gpj_index *out,
+                    void *stream);
+
+/* Same build into caller-owned buffers (index->d_string, d_leveled,
+ * d_newline with newline_capacity entries, optional d_escape/d_quote).
+ * Asynchronous: the line count, final string state and final depth are
+ * written to d_summary[0..2] (3 x uint64 in device memory).  Scratch comes
+ * from the context.  If the newline count exceeds newline_capacity - 1 the
+ * extra offsets are dropped; d_summary[0] still holds the true line count.
+ * Replaces the same builders as gpj_index_build. */
+int gpj_index_build_async(gpj_ctx *ctx, const uint8_t *d_input,
+                          uint64_t size_bytes, int num_levels, uint32_t flags,
+                          gpj_index *index, uint64_t *d_summary, void *stream);
+
+/* Releases what gpj_index_build allocated. */
+int gpj_index_free(gpj_ctx *ctx, gpj_index *index);
+
+/* Runs one compiled query over every record of an indexed partition and
+ * writes int32 (start, end) pairs, partition-local, -1 = no match, into
+ * d_out[num_lines][num_result_slots][2].  Asynchronous on `stream`.
+ * Replaces the per-query launch of query::kernels::orig::execute_batch
+ * (src/gpjson/query/kernels/orig/query_executor_host.cu:179-237) and the
+ * query kernel (src/gpjson/query/kernels/orig/query.cu:144-454). */
+int gpj_query_run(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
+                  uint64_t ir_len, uint32_t num_result_slots, int32_t *d_out,
+                  void *stream);
+
+/* As gpj_query_run with int64 offsets, for partitions of 2 GiB and more
+ * (the reference narrows sizes to int, query_executor_host.cu:28-33). */
+int gpj_query_run64(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
+                    uint64_t ir_len, uint32_t num_result_slots, int64_t *d_out,
+                    void *stream);
+
+/* Options of gpj_query_run_opts; all-zero means the reference behaviour
+ * (int32 offsets, records are lines, query level 0 = bitmap level 0). */
+typedef struct gpj_query_opts {
+  uint32_t base_level;   /* bitmap level that query level 0 maps to: 1 makes
+                            the elements of a top-level array the records
+                            ("$[*]..." queries) */
+  uint32_t offset_bytes; /* 4 (int32, default when 0) or 8 (int64) */
+  uint32_t reserved[2];
+} gpj_query_opts;
+
+/* gpj_query_run with options (record level, offset width).  Same kernel and
+ * replaced interface as gpj_query_run; the array-element records extend the
+ * reference, whose compiler rejects "[*]" (query_compiler.cpp:287-289). */
+int gpj_query_run_opts(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
+                       uint64_t ir_len, uint32_t num_result_slots,
+                       const gpj_query_opts *opts, void *d_out, void *stream);
+
+/* End to end from host memory: copies h_input to the device, builds the
+ * index with num_levels levels, runs the queries and copies the int32 result
+ * arrays back.  h_out[q] must hold out_capacity[q] int32; *num_lines gets
+ * the record count (0 for an empty input).  base_levels may be NULL (all 0).  GPJ_ERR_CAPACITY (nothing copied back) if a result does
+ * not fit.  Replaces the per-partition body of gpjson::Engine::query
+ * (src/gpjson/engine.cpp:131-166: load_to_device, build, execute_batch). */
+int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes,
+                   int num_levels, uint32_t num_queries,
+                   const uint8_t *const *h_irs, const uint64_t *ir_lens,
+                   const uint32_t *num_result_slots, const uint32_t *base_levels,
+                   int32_t *const *h_out, const uint64_t *out_capacity,
+                   uint64_t *num_lines, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPJSON_B200_H */

@@ -1,0 +1,518 @@
+/*
+ * CPU oracle for the GpJSON structural index and JSONPath query path.
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference arm of bench.py as the checker and the CPU
+ * baseline.  The product library never links or calls it.
+ *
+ * The code below is a plain, byte-serial restatement of the reference
+ * (Xinyu-Li-123/15418-project).  Each function names the reference lines it
+ * follows; where the reference reads out of bounds on malformed input (its
+ * release build compiles the asserts out), this restatement reads a 0 byte
+ * instead, and says so at that spot.
+ */
+#include "gpjson_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+uint64_t orc_num_words(uint64_t n) { return (n + 63u) / 64u; }
+
+/* tests/index/newline_index_test.cpp:27-35 (expected_newline_index) and
+ * src/gpjson/index/sharemem_index_builder.cu:343-349 (num_lines = count + 1,
+ * slot 0 = 0). */
+uint64_t orc_newline_index(const uint8_t *in, uint64_t n, int64_t *out,
+                           uint64_t cap) {
+  uint64_t lines = 1;
+  if (cap > 0) out[0] = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (in[i] == '\n') {
+      if (lines < cap) out[lines] = (int64_t)i;
+      ++lines;
+    }
+  }
+  return lines;
+}
+
+/* Escape bitmap with the SHAREMEM word-local carry:
+ *  - carry into word w is the parity of the trailing '\\' run inside word w-1
+ *    only, read backward from its last in-file byte
+ *    (src/gpjson/index/kernels/sharemem/uncombined/escape-carry-index.cu:95-164);
+ *  - inside a word the state machine is "bit i = carry; carry = (byte=='\\')
+ *    ? !carry : 0" (sharemem/uncombined/escape-index.cu:29-96).
+ * An all-backslash word therefore passes carry 0 on, whatever came before. */
+void orc_escape_index(const uint8_t *in, uint64_t n, uint64_t *E) {
+  const uint64_t W = orc_num_words(n);
+  for (uint64_t w = 0; w < W; ++w) {
+    int carry = 0;
+    if (w > 0) {
+      /* backward read of word w-1 (always a full word) */
+      const uint64_t base = (w - 1) * 64u;
+      for (int b = 63; b >= 0; --b) {
+        if (in[base + (uint64_t)b] == '\\') carry ^= 1;
+        else break;
+      }
+    }
+    uint64_t word = 0;
+    const uint64_t base = w * 64u;
+    for (int b = 0; b < 64 && base + (uint64_t)b < n; ++b) {
+      if (carry) word |= (uint64_t)1 << b;
+      carry = (in[base + (uint64_t)b] == '\\') ? !carry : 0;
+    }
+    E[w] = word;
+  }
+}
+
+/* tests/index/string_index_test.cpp:28-34 counts the whole preceding run. */
+void orc_escape_index_unbounded(const uint8_t *in, uint64_t n, uint64_t *E) {
+  const uint64_t W = orc_num_words(n);
+  memset(E, 0, W * sizeof(uint64_t));
+  int carry = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (carry) E[i / 64u] |= (uint64_t)1 << (i % 64u);
+    carry = (in[i] == '\\') ? !carry : 0;
+  }
+}
+
+/* sharemem/quote-index.cu:29-95: Q bit = '"' and not escaped. */
+void orc_quote_index(const uint8_t *in, uint64_t n, const uint64_t *E,
+                     uint64_t *Q) {
+  const uint64_t W = orc_num_words(n);
+  for (uint64_t w = 0; w < W; ++w) {
+    uint64_t word = 0;
+    for (int b = 0; b < 64 && w * 64u + (uint64_t)b < n; ++b) {
+      const uint64_t bit = (uint64_t)1 << b;
+      if (in[w * 64u + (uint64_t)b] == '"' && (E[w] & bit) == 0) word |= bit;
+    }
+    Q[w] = word;
+  }
+}
+
+/* sharemem_index_builder.cu:206-217 (inclusive XOR scan of per-word quote
+ * parity) + sharemem/string-index.cu:3-31 (shift-xor cascade, then xor with
+ * all ones when the carried parity is 1).  Bits past the end of the data keep
+ * the in-string state at the end, exactly like the cascade does. */
+void orc_string_index(const uint64_t *Q, uint64_t W, uint64_t *S) {
+  uint64_t state = 0; /* 0 or all ones */
+  for (uint64_t w = 0; w < W; ++w) {
+    uint64_t x = Q[w];
+    uint64_t out = 0;
+    for (int b = 0; b < 64; ++b) {
+      if ((x >> b) & 1u) state = ~state;
+      out |= (state & 1u) << b;
+    }
+    S[w] = out;
+  }
+}
+
+/* sharemem/leveled-bitmaps-carry-index.cu:202-277 + the char scan of
+ * sharemem_index_builder.cu:281-301 + sharemem/leveled-bitmaps-index.cu:210-316
+ * collapse into one running signed-char depth that starts at -1 and wraps
+ * modulo 256.  Per byte outside strings:
+ *   '{' '['  -> depth++, then set bit at level depth
+ *   '}' ']'  -> set bit at level depth, then depth--
+ *   ':' ','  -> set bit at level depth
+ * and a bit is stored only when 0 <= depth < num_levels
+ * (also tests/index/leveled_bitmap_index_test.cpp:57-92). */
+void orc_leveled_bitmap_index(const uint8_t *in, uint64_t n, const uint64_t *S,
+                              int num_levels, uint64_t *LB) {
+  const uint64_t W = orc_num_words(n);
+  memset(LB, 0, W * (uint64_t)num_levels * sizeof(uint64_t));
+  int8_t level = -1;
+  for (uint64_t i = 0; i < n; ++i) {
+    const uint64_t w = i / 64u;
+    const uint64_t bit = (uint64_t)1 << (i % 64u);
+    if (S[w] & bit) continue;
+    const uint8_t c = in[i];
+    if (c == '{' || c == '[') {
+      level = (int8_t)(level + 1);
+      if (level >= 0 && level < num_levels) LB[(uint64_t)level * W + w] |= bit;
+    } else if (c == '}' || c == ']') {
+      if (level >= 0 && level < num_levels) LB[(uint64_t)level * W + w] |= bit;
+      level = (int8_t)(level - 1);
+    } else if (c == ':' || c == ',') {
+      if (level >= 0 && level < num_levels) LB[(uint64_t)level * W + w] |= bit;
+    }
+  }
+}
+
+uint64_t orc_build_index(const uint8_t *in, uint64_t n, int num_levels,
+                         uint64_t *E, uint64_t *Q, uint64_t *S, uint64_t *LB,
+                         int64_t *NL, uint64_t nl_cap) {
+  const uint64_t W = orc_num_words(n);
+  uint64_t *e = E;
+  uint64_t *tmp = 0;
+  if (e == 0) {
+    tmp = (uint64_t *)malloc((W ? W : 1) * sizeof(uint64_t));
+    e = tmp;
+  }
+  /* Q goes into the S buffer when not requested, as the reference does
+   * (sharemem_index_builder.cu:194-197); the scan below reads word w before
+   * writing it, so it runs in place. */
+  uint64_t *q = Q ? Q : S;
+  orc_escape_index(in, n, e);
+  orc_quote_index(in, n, e, q);
+  orc_string_index(q, W, S);
+  orc_leveled_bitmap_index(in, n, S, num_levels, LB);
+  free(tmp);
+  return orc_newline_index(in, n, NL, nl_cap);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Query interpreter: src/gpjson/query/kernels/orig/query.cu:144-454         */
+/* ------------------------------------------------------------------------ */
+
+enum {
+  OP_END = 0x00,
+  OP_STORE_RESULT = 0x01,
+  OP_MOVE_UP = 0x02,
+  OP_MOVE_DOWN = 0x03,
+  OP_MOVE_TO_KEY = 0x04,
+  OP_MOVE_TO_INDEX = 0x05,
+  OP_MOVE_TO_INDEX_REVERSE = 0x06,
+  OP_MARK_POSITION = 0x07,
+  OP_RESET_POSITION = 0x08,
+  OP_EXPRESSION_STRING_EQUALS = 0x09
+};
+#define ORC_MAX_LEVELS 16 /* query.cu:20 MAX_NUM_LEVELS */
+
+typedef struct {
+  const uint8_t *in;
+  int64_t n;
+  const uint64_t *S;
+  const uint64_t *LB;
+  int64_t W;
+  const uint8_t *ir;
+  int64_t ir_len;
+  int levels; /* levels held by LB */
+  int base;   /* bitmap level of query level 0 */
+} qctx;
+
+/* The reference indexes file[] without bounds checks; on well-formed JSON it
+ * never leaves the partition.  Here a read outside [0, n) yields 0. */
+static inline uint8_t at(const qctx *c, int64_t i) {
+  return (i >= 0 && i < c->n) ? c->in[i] : 0;
+}
+static inline uint64_t word_at(const uint64_t *bm, int64_t W, int64_t i) {
+  return (i >= 0 && i < W) ? bm[i] : 0;
+}
+static inline uint8_t ir_at(const qctx *c, int64_t i) {
+  return (i >= 0 && i < c->ir_len) ? c->ir[i] : 0;
+}
+
+/* query.cu:34-37 */
+static inline uint64_t mask_through_bit(int bit_offset) {
+  return bit_offset == 63 ? ~(uint64_t)0 : (((uint64_t)1 << (bit_offset + 1)) - 1);
+}
+
+static inline int clz64(uint64_t x) { return __builtin_clzll(x); }
+static inline int ffs64(uint64_t x) { return __builtin_ffsll((long long)x); }
+
+/* query.cu:39-77 find_previous_bitmap_bit */
+static int64_t find_previous_bitmap_bit(const uint64_t *bitmap, int64_t W,
+                                        int64_t min_index, int64_t line_index) {
+  if (line_index < min_index) return -1;
+  int64_t word_index = line_index / 64;
+  int64_t word_base = word_index * 64;
+  uint64_t word = word_at(bitmap, W, word_index);
+  word &= mask_through_bit((int)(line_index - word_base));
+  while (word_base + 63 >= min_index) {
+    uint64_t candidate = word;
+    const int64_t first_bit = min_index - word_base;
+    if (first_bit > 0) candidate &= ~mask_through_bit((int)(first_bit - 1));
+    if (candidate != 0) return word_base + 63 - clz64(candidate);
+    if (word_index == 0) break;
+    --word_index;
+    word_base -= 64;
+    if (word_base + 63 < min_index) break;
+    word = word_at(bitmap, W, word_index);
+  }
+  return -1;
+}
+
+/* query.cu:79-115 find_next_structural_char */
+static int64_t find_next_structural_char(const qctx *c, int64_t level_end,
+                                         int64_t line_index, int level) {
+  if (line_index >= level_end) return level_end;
+  if (level + c->base < 0 || level + c->base >= c->levels) return level_end;
+  const uint64_t *lvl = c->LB + (uint64_t)c->W * (uint64_t)(level + c->base);
+  int64_t word_index = line_index / 64;
+  int64_t word_base = word_index * 64;
+  uint64_t word = word_at(lvl, c->W, word_index);
+  word &= ~(uint64_t)0 << (line_index - word_base);
+  while (word_base <= level_end) {
+    uint64_t candidate = word;
+    const int64_t last_bit = level_end - word_base;
+    if (last_bit < 63) candidate &= mask_through_bit((int)last_bit);
+    if (candidate != 0) return word_base + ffs64(candidate) - 1;
+    ++word_index;
+    word_base += 64;
+    if (word_base > level_end) break;
+    word = word_at(lvl, c->W, word_index);
+  }
+  return level_end;
+}
+
+/* query.cu:117-128 find_previous_structural_char */
+static int64_t find_previous_structural_char(const qctx *c, int64_t level_start,
+                                             int64_t line_index, int level) {
+  if (line_index <= level_start) return level_start;
+  if (level + c->base < 0 || level + c->base >= c->levels) return level_start;
+  const uint64_t *lvl = c->LB + (uint64_t)c->W * (uint64_t)(level + c->base);
+  const int64_t s = find_previous_bitmap_bit(lvl, c->W, level_start, line_index);
+  return s == -1 ? level_start : s;
+}
+
+/* query.cu:130-140 read_varint (int arithmetic, LEB128) */
+static int read_varint(const qctx *c, int64_t *pos) {
+  int value = 0, shift = 0, byte = 0;
+  while (((byte = ir_at(c, (*pos)++)) & 0x80) != 0) {
+    value |= (byte & 0x7F) << shift;
+    shift += 7;
+    if (shift > 28) break; /* the reference asserts shift <= 35 */
+  }
+  return value | (byte << shift);
+}
+
+/* One record: query.cu:150-451.  out points at this record's 2*num_results
+ * slots, already filled with -1. */
+static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
+                         int num_results, int64_t *out) {
+  if (line_start < 0 || line_start >= c->n || line_end < 0) return;
+  if (line_end >= c->n) line_end = c->n - 1;
+  while (line_end > line_start && at(c, line_end) != '}') --line_end;
+  while (line_start < line_end && at(c, line_start) != '{') ++line_start;
+  if (line_start == line_end) return;
+
+  int64_t line_index = line_start;
+  int current_level = 0;
+  int64_t query_pos = 0;
+  int64_t level_end[ORC_MAX_LEVELS];
+  level_end[0] = line_end;
+  for (int i = 1; i < ORC_MAX_LEVELS; ++i) level_end[i] = -1;
+  int64_t marked_pos[ORC_MAX_LEVELS];
+  int marked_pos_level[ORC_MAX_LEVELS];
+  int marked_pos_index = -1;
+  int num_results_index = 0;
+  int64_t key_pos = 0;
+  int key_len = 0;
+  int target_index = 0;
+  int64_t curr_index[ORC_MAX_LEVELS];
+  for (int i = 0; i < ORC_MAX_LEVELS; ++i) curr_index[i] = -1;
+
+/* The reference has no guard for these; the compiler never emits IR that
+ * reaches them.  Leaving the record keeps the restatement memory safe. */
+#define LEVEL_OK(l) ((l) >= 0 && (l) < ORC_MAX_LEVELS)
+
+  for (;;) {
+    const uint8_t op = ir_at(c, query_pos++);
+    switch (op) {
+    case OP_END:
+      return;
+
+    case OP_STORE_RESULT: { /* query.cu:213-231 */
+      if (!LEVEL_OK(current_level)) return;
+      int64_t end_str = level_end[current_level];
+      while (at(c, line_index) == ' ' && line_index < level_end[current_level])
+        ++line_index;
+      while (end_str > line_index && at(c, end_str - 1) == ' ') --end_str;
+      if (num_results_index < num_results) {
+        out[num_results_index * 2] = line_index;
+        out[num_results_index * 2 + 1] = end_str;
+      }
+      ++num_results_index;
+      break;
+    }
+
+    case OP_MOVE_UP: /* query.cu:233-237 */
+      if (!LEVEL_OK(current_level)) return;
+      line_index = level_end[current_level];
+      level_end[current_level] = -1;
+      --current_level;
+      break;
+
+    case OP_MOVE_DOWN: /* query.cu:239-252 */
+      ++current_level;
+      if (!LEVEL_OK(current_level) || current_level < 1) return;
+      if (level_end[current_level] == -1) {
+        level_end[current_level] = find_next_structural_char(
+            c, level_end[current_level - 1], line_index + 1, current_level - 1);
+        while (at(c, line_index) == ' ') ++line_index;
+      }
+      break;
+
+    case OP_MOVE_TO_KEY: /* query.cu:254-302 */
+      key_len = read_varint(c, &query_pos);
+      key_pos = query_pos;
+      query_pos += key_len;
+      if (!LEVEL_OK(current_level)) return;
+      if (at(c, line_index) == '{') {
+        for (;;) { /* search_key */
+          ++line_index;
+          line_index = find_next_structural_char(c, level_end[current_level],
+                                                 line_index, current_level);
+          if (at(c, line_index) == ':') {
+            const int64_t string_end = find_previous_bitmap_bit(
+                c->S, c->W, line_start + 1, line_index - 1);
+            const int64_t string_start = string_end - key_len;
+            int mismatch = 0;
+            if (string_start < line_start || at(c, string_start) != '"') {
+              mismatch = 1;
+            } else {
+              for (int i = 0; i < key_len; ++i) {
+                if (ir_at(c, key_pos + i) != at(c, string_start + i + 1)) {
+                  mismatch = 1;
+                  break;
+                }
+              }
+            }
+            if (mismatch) {
+              ++line_index;
+              line_index = find_next_structural_char(
+                  c, level_end[current_level], line_index, current_level);
+              if (at(c, line_index) == '}') return;
+              continue; /* goto search_key */
+            }
+          }
+          break;
+        }
+        ++line_index;
+      } else {
+        return;
+      }
+      break;
+
+    case OP_MOVE_TO_INDEX: /* query.cu:304-346 */
+      target_index = read_varint(c, &query_pos);
+      if (!LEVEL_OK(current_level)) return;
+      {
+        const uint8_t ch = at(c, line_index);
+        if (ch == '[' || ch == ',' || ch == ']') {
+          if (ch == '[') curr_index[current_level] = 0;
+          else ++curr_index[current_level];
+          for (;;) { /* search_index */
+            if (curr_index[current_level] < target_index) {
+              ++line_index;
+              line_index = find_next_structural_char(
+                  c, level_end[current_level], line_index, current_level);
+              if (at(c, line_index) == ',') {
+                ++curr_index[current_level];
+                continue;
+              }
+              return;
+            }
+            if (curr_index[current_level] > target_index) {
+              --line_index;
+              line_index =
+                  find_previous_structural_char(c, 0, line_index, current_level);
+              --curr_index[current_level];
+              continue;
+            }
+            break;
+          }
+          if (at(c, line_index) == ']') return;
+          ++line_index;
+        } else {
+          return;
+        }
+      }
+      break;
+
+    case OP_MOVE_TO_INDEX_REVERSE: /* query.cu:348-392 */
+      target_index = read_varint(c, &query_pos);
+      if (!LEVEL_OK(current_level)) return;
+      line_index = level_end[current_level] - 1;
+      while (at(c, line_index) == ' ') --line_index;
+      {
+        const uint8_t ch = at(c, line_index);
+        if (ch == ']' || ch == ',' || ch == '[') {
+          if (ch == ']') curr_index[current_level] = 0;
+          else ++curr_index[current_level];
+          for (;;) { /* search_index_reverse */
+            if (curr_index[current_level] < target_index) {
+              --line_index;
+              line_index =
+                  find_previous_structural_char(c, 0, line_index, current_level);
+              if (at(c, line_index) == ',' ||
+                  curr_index[current_level] + 1 == target_index) {
+                ++curr_index[current_level];
+                continue;
+              }
+              return;
+            }
+            if (curr_index[current_level] > target_index) {
+              ++line_index;
+              line_index = find_next_structural_char(
+                  c, level_end[current_level], line_index, current_level);
+              --curr_index[current_level];
+              continue;
+            }
+            break;
+          }
+          ++line_index;
+        } else {
+          return;
+        }
+      }
+      break;
+
+    case OP_MARK_POSITION: /* query.cu:394-399 */
+      if (marked_pos_index + 1 >= ORC_MAX_LEVELS) return;
+      ++marked_pos_index;
+      marked_pos[marked_pos_index] = line_index;
+      marked_pos_level[marked_pos_index] = current_level;
+      break;
+
+    case OP_RESET_POSITION: /* query.cu:401-412 */
+      if (marked_pos_index < 0) return;
+      line_index = marked_pos[marked_pos_index];
+      current_level = marked_pos_level[marked_pos_index];
+      --marked_pos_index;
+      for (int i = current_level + 1; i < ORC_MAX_LEVELS; ++i) {
+        if (i < 0) continue;
+        if (level_end[i] == -1) break;
+        level_end[i] = -1;
+      }
+      break;
+
+    case OP_EXPRESSION_STRING_EQUALS: /* query.cu:414-441 */
+      key_len = read_varint(c, &query_pos);
+      key_pos = query_pos;
+      query_pos += key_len;
+      if (!LEVEL_OK(current_level)) return;
+      while (at(c, line_index) == ' ' && line_index < level_end[current_level])
+        ++line_index;
+      {
+        int64_t string_end = level_end[current_level] - 1;
+        while (line_index < string_end && at(c, string_end) == ' ') --string_end;
+        const int64_t string_length = string_end - line_index + 1;
+        if (string_length != key_len) return;
+        for (int i = 0; i < key_len; ++i) {
+          if (ir_at(c, key_pos + i) != at(c, line_index + i)) return;
+        }
+      }
+      break;
+
+    default: /* the reference asserts; release builds fall through */
+      break;
+    }
+    if (query_pos > c->ir_len + 1) return; /* ran off the IR */
+  }
+#undef LEVEL_OK
+}
+
+int orc_query(const uint8_t *in, uint64_t n, const int64_t *NL,
+              uint64_t num_lines, const uint64_t *S, const uint64_t *LB,
+              uint64_t W, int num_levels, int base_level, const uint8_t *ir,
+              uint64_t ir_len, int num_results, int64_t *out) {
+  qctx c = {in, (int64_t)n, S, LB, (int64_t)W, ir, (int64_t)ir_len, num_levels, base_level};
+  for (uint64_t r = 0; r < num_lines; ++r) {
+    int64_t *o = out + r * (uint64_t)num_results * 2u;
+    for (int i = 0; i < 2 * num_results; ++i) o[i] = -1;
+    if (n == 0) continue;
+    const int64_t line_start = NL[r];
+    const int64_t line_end = (r + 1 < num_lines) ? NL[r + 1] : (int64_t)n - 1;
+    query_record(&c, line_start, line_end, num_results, o);
+  }
+  return 0;
+}

@@ -1,0 +1,140 @@
+"""Query kernel on the GPU vs the CPU oracle: bit-exact (start, end) result
+arrays, plus the reference's own query known answers."""
+import json
+import random
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from devmem import to_device
+
+pytestmark = pytest.mark.gpu
+KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
+
+TWEET_QUERIES = [
+    "$.user.lang", "$.lang", '$.user.lang[?(@ == "nl")]', '$.user.lang[?(@ == "en")]',
+    "$.entities.hashtags[0:8].text", "$.place.country_code", "$.retweeted_status.user.id",
+    "$.entities.hashtags[-1].text", "$.entities.hashtags[-2:]", "$.coordinates.coordinates[1]",
+    "$['user']['name']", "$.entities.urls[0,1].url", "$.place.bounding_box.coordinates[0][2][1]",
+    "$.retweeted_status.entities.hashtags[1].indices[0]", "$.user", "$.nonexistent.key",
+]
+
+
+def run_gpu(ctx, gpj, data, queries, wide=False, levels=None):
+    b = oracle.as_bytes(data)
+    comp = [gpj.compile(q) for q in queries]
+    L = levels or max(c.max_depth for c in comp)
+    t, ptr = to_device(b)
+    ix = ctx.build_index(ptr, b.size, L)
+    outs = []
+    try:
+        for c in comp:
+            dt = torch.int64 if wide else torch.int32
+            out = torch.full((max(1, ix.num_lines * c.num_result_slots * 2),), -7, dtype=dt,
+                             device="cuda")
+            ctx.query(ix, c, out.data_ptr(), wide=wide)
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy()[: ix.num_lines * c.num_result_slots * 2]
+                        .reshape(ix.num_lines, c.num_result_slots, 2))
+    finally:
+        ctx.free_index(ix)
+    return comp, L, outs
+
+
+def check_against_oracle(ctx, gpj, data, queries, wide=False):
+    comp, L, outs = run_gpu(ctx, gpj, data, queries, wide)
+    want_ix = oracle.OracleIndex(data, L)
+    for c, got in zip(comp, outs):
+        want = want_ix.query(c.ir_bytes, c.num_result_slots)
+        if b := oracle.as_bytes(data).size:
+            np.testing.assert_array_equal(got.astype(np.int64), want, err_msg=c.query_text)
+    return comp, outs
+
+
+def texts(data: bytes, res):
+    return [[data[s:e].decode() for s, e in line if s >= 0] for line in res]
+
+
+def test_query_executor_kats(cuda_ctx, gpj):
+    k = KATS["query_executor"]
+    data = k["json_text"].encode()
+    comp, outs = check_against_oracle(cuda_ctx, gpj, data, k["queries"])
+    for qi, expected in k["expected"].items():
+        assert texts(data, outs[int(qi)]) == [[expected]]
+    assert texts(data, outs[k["queries"].index(k["unmatched_query"])]) == [[]]
+
+
+def test_engine_kats(cuda_ctx, gpj):
+    k = KATS["engine"]
+    data = k["contents"].encode()
+    comp, outs = check_against_oracle(cuda_ctx, gpj, data, k["queries"])
+    for q, line, expected in k["expected"]:
+        assert texts(data, outs[q])[line] == [expected]
+
+
+@pytest.mark.parametrize("wide", [False, True], ids=["int32", "int64"])
+def test_tweets_many_queries(cuda_ctx, gpj, wide):
+    from gpjson_b200 import datagen
+    data = datagen.tweets(11, 8 << 20)
+    check_against_oracle(cuda_ctx, gpj, data, TWEET_QUERIES, wide)
+
+
+def test_products_lines(cuda_ctx, gpj):
+    from gpjson_b200 import datagen
+    data = datagen.products(2, 8 << 20)
+    check_against_oracle(cuda_ctx, gpj, data, ["$.categoryPath[1:3].id", "$.offers[0].type[1]",
+                                               "$.shipping.ground", "$.sku"])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_garbage_input_matches_oracle(cuda_ctx, gpj, seed):
+    rng = random.Random(seed)
+    alphabet = b'{}[]:,"\\\n ab'
+    data = bytes(rng.choices(alphabet, weights=[6, 6, 3, 3, 5, 5, 8, 1, 2, 3, 8, 8], k=20000))
+    check_against_oracle(cuda_ctx, gpj, data, ["$.a", "$.a.b", "$.b[1]", "$.a[-1]",
+                                               '$.a[?(@ == "b")]', "$.a[0:3].b"])
+
+
+def test_query_host_end_to_end(cuda_ctx, gpj):
+    from gpjson_b200 import datagen
+    data = datagen.tweets(4, 2 << 20)
+    comp = [gpj.compile(q) for q in ["$.user.lang", "$.entities.hashtags[0:8].text"]]
+    L = max(c.max_depth for c in comp)
+    lines = data.tobytes().count(b"\n") + 1
+    host_in = torch.from_numpy(data.copy()).pin_memory()
+    outs = [torch.empty(lines * c.num_result_slots * 2, dtype=torch.int32).pin_memory()
+            for c in comp]
+    got_lines = cuda_ctx.query_host(host_in.data_ptr(), data.size, L, comp,
+                                    [o.data_ptr() for o in outs], [o.numel() for o in outs])
+    assert got_lines == lines
+    want = oracle.OracleIndex(data, L)
+    for c, o in zip(comp, outs):
+        np.testing.assert_array_equal(o.numpy().astype(np.int64).reshape(lines, -1, 2),
+                                      want.query(c.ir_bytes, c.num_result_slots))
+
+
+@pytest.mark.parametrize("query", ["$.categoryPath[1:3].id", "$.offers[0].type[1]", "$.sku",
+                                   "$.categoryPath[*].name"])
+def test_array_element_records(cuda_ctx, gpj, query):
+    """$[*].X: the elements of the top-level array are the records (query
+    level 0 = bitmap level 1)."""
+    from gpjson_b200 import datagen
+    data = datagen.products(2, 8 << 20)
+    c = gpj.compile(query, wildcard_limit=6)
+    L = c.max_depth + 1
+    t, ptr = to_device(data)
+    ix = cuda_ctx.build_index(ptr, data.size, L)
+    try:
+        out = torch.full((ix.num_lines * c.num_result_slots * 2,), -7, dtype=torch.int32,
+                         device="cuda")
+        cuda_ctx.query(ix, c, out.data_ptr(), base_level=1)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().astype(np.int64).reshape(ix.num_lines, -1, 2)
+    finally:
+        cuda_ctx.free_index(ix)
+    want = oracle.OracleIndex(data, L).query(c.ir_bytes, c.num_result_slots, 1)
+    np.testing.assert_array_equal(got, want)
+    assert (got[1:-1, 0, 0] >= 0).mean() > 0.5  # most elements match slot 0
