@@ -107,15 +107,18 @@ __device__ int64_t prev_struct(const Rec &c, int64_t level_start,
   return s == -1 ? level_start : s;
 }
 
-// query.cu:130-140 (LEB128, int arithmetic)
+// query.cu:130-140 (LEB128).  Unsigned arithmetic reinterpreted as int, as
+// the reference's int result wraps; an operand longer than five bytes (never
+// produced by the compiler) reads as -1.
 __device__ int read_varint(const Rec &c, int64_t &pos) {
-  int value = 0, shift = 0, byte = 0;
-  while (((byte = ir_at(c, pos++)) & 0x80) != 0) {
-    value |= (byte & 0x7F) << shift;
+  uint32_t value = 0, byte = 0;
+  int shift = 0;
+  while (((byte = ir_at(c, pos++)) & 0x80u) != 0) {
+    value |= (byte & 0x7Fu) << shift;
     shift += 7;
-    if (shift > 28) break;
+    if (shift > 28) return -1;
   }
-  return value | (byte << shift);
+  return int(value | (byte << shift));
 }
 
 template <typename OutT>
@@ -130,6 +133,12 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
   int64_t line_index = line_start;
   int level = 0;
   int64_t qp = 0;
+  // Step bound of one search loop.  On well-formed JSON every step lands on a
+  // new structural character of the record, so the bound is never reached;
+  // on malformed input the reference's loops can revisit the same character
+  // forever, and the record is abandoned instead.
+  const int64_t max_steps = (line_end - line_start) + 2;
+  int64_t steps = 0;
   int64_t level_end[kMaxQueryLevels];
   level_end[0] = line_end;
 #pragma unroll
@@ -181,9 +190,11 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       key_len = read_varint(c, qp);
       key_pos = qp;
       qp += key_len;
-      if (!LEVEL_OK(level)) return;
+      if (key_len < 0 || !LEVEL_OK(level)) return;
       if (at(c, line_index) != '{') return;
+      steps = 0;
       for (;;) {
+        if (++steps > max_steps) return;
         ++line_index;
         line_index = next_struct(c, level_end[level], line_index, level);
         if (at(c, line_index) == ':') {
@@ -211,7 +222,9 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       if (ch != '[' && ch != ',' && ch != ']') return;
       if (ch == '[') curr_index[level] = 0;
       else ++curr_index[level];
+      steps = 0;
       for (;;) {
+        if (++steps > max_steps) return;
         if (curr_index[level] < target) {
           ++line_index;
           line_index = next_struct(c, level_end[level], line_index, level);
@@ -242,7 +255,9 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       if (ch != ']' && ch != ',' && ch != '[') return;
       if (ch == ']') curr_index[level] = 0;
       else ++curr_index[level];
+      steps = 0;
       for (;;) {
+        if (++steps > max_steps) return;
         if (curr_index[level] < target) {
           --line_index;
           line_index = prev_struct(c, 0, line_index, level);
@@ -284,7 +299,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       key_len = read_varint(c, qp);
       key_pos = qp;
       qp += key_len;
-      if (!LEVEL_OK(level)) return;
+      if (key_len < 0 || !LEVEL_OK(level)) return;
       while (at(c, line_index) == ' ' && line_index < level_end[level]) ++line_index;
       int64_t string_end = level_end[level] - 1;
       while (line_index < string_end && at(c, string_end) == ' ') --string_end;

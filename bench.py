@@ -337,9 +337,10 @@ def cpu_baseline(data, comp, records, levels, budget_s: float, threads: int | No
     def work(ab):
         a, b = ab
         ix = oracle.OracleIndex(data[a:b], levels)
-        for c, _base in comp:
-            if _base == 0:
-                ix.query(c.ir_bytes, c.num_result_slots)
+        for c, base in comp:
+            # a partition cut out of a top-level array holds its elements at
+            # depth 0, except the first one, which holds the opening bracket
+            ix.query(c.ir_bytes, c.num_result_slots, base if a == 0 else 0)
         return b - a
 
     t0 = time.perf_counter()

@@ -263,15 +263,18 @@ static int64_t find_previous_structural_char(const qctx *c, int64_t level_start,
   return s == -1 ? level_start : s;
 }
 
-/* query.cu:130-140 read_varint (int arithmetic, LEB128) */
+/* query.cu:130-140 read_varint (LEB128).  Unsigned arithmetic reinterpreted
+ * as int, as the reference's int result wraps; an operand longer than five
+ * bytes (never produced by the compiler) reads as -1. */
 static int read_varint(const qctx *c, int64_t *pos) {
-  int value = 0, shift = 0, byte = 0;
-  while (((byte = ir_at(c, (*pos)++)) & 0x80) != 0) {
-    value |= (byte & 0x7F) << shift;
+  uint32_t value = 0, byte = 0;
+  int shift = 0;
+  while (((byte = ir_at(c, (*pos)++)) & 0x80u) != 0) {
+    value |= (byte & 0x7Fu) << shift;
     shift += 7;
-    if (shift > 28) break; /* the reference asserts shift <= 35 */
+    if (shift > 28) return -1;
   }
-  return value | (byte << shift);
+  return (int)(value | (byte << shift));
 }
 
 /* One record: query.cu:150-451.  out points at this record's 2*num_results
@@ -287,6 +290,12 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
   int64_t line_index = line_start;
   int current_level = 0;
   int64_t query_pos = 0;
+  /* Step bound of one search loop (not in the reference): on well-formed JSON
+   * each step lands on a new structural character of the record, so it is
+   * never reached; on malformed input the reference's loops can revisit one
+   * character forever, and the record is abandoned instead. */
+  const int64_t max_steps = (line_end - line_start) + 2;
+  int64_t steps = 0;
   int64_t level_end[ORC_MAX_LEVELS];
   level_end[0] = line_end;
   for (int i = 1; i < ORC_MAX_LEVELS; ++i) level_end[i] = -1;
@@ -345,9 +354,11 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
       key_len = read_varint(c, &query_pos);
       key_pos = query_pos;
       query_pos += key_len;
-      if (!LEVEL_OK(current_level)) return;
+      if (key_len < 0 || !LEVEL_OK(current_level)) return;
       if (at(c, line_index) == '{') {
+        steps = 0;
         for (;;) { /* search_key */
+          if (++steps > max_steps) return;
           ++line_index;
           line_index = find_next_structural_char(c, level_end[current_level],
                                                  line_index, current_level);
@@ -390,7 +401,9 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
         if (ch == '[' || ch == ',' || ch == ']') {
           if (ch == '[') curr_index[current_level] = 0;
           else ++curr_index[current_level];
+          steps = 0;
           for (;;) { /* search_index */
+            if (++steps > max_steps) return;
             if (curr_index[current_level] < target_index) {
               ++line_index;
               line_index = find_next_structural_char(
@@ -428,7 +441,9 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
         if (ch == ']' || ch == ',' || ch == '[') {
           if (ch == ']') curr_index[current_level] = 0;
           else ++curr_index[current_level];
+          steps = 0;
           for (;;) { /* search_index_reverse */
+            if (++steps > max_steps) return;
             if (curr_index[current_level] < target_index) {
               --line_index;
               line_index =
@@ -479,7 +494,7 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
       key_len = read_varint(c, &query_pos);
       key_pos = query_pos;
       query_pos += key_len;
-      if (!LEVEL_OK(current_level)) return;
+      if (key_len < 0 || !LEVEL_OK(current_level)) return;
       while (at(c, line_index) == ' ' && line_index < level_end[current_level])
         ++line_index;
       {
