@@ -273,7 +273,15 @@ __global__ void __launch_bounds__(kIndexThreads)
   const int lane = tid & 31;
   const int warp = tid >> 5;
 
-  if (tid == 0) s_tile_id = atomicAdd(P.tile_counter, 1u);
+  if (tid == 0) {
+    s_tile_id = atomicAdd(P.tile_counter, 1u);
+    if constexpr (kTma) {
+      // the barrier must be initialised before any thread polls it: shared
+      // memory may still hold a barrier of an earlier CTA on this SM
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+  }
   __syncthreads();
   const uint32_t tile = s_tile_id;
   if (tile >= P.num_tiles) return;  // cannot happen with grid == num_tiles
@@ -284,8 +292,6 @@ __global__ void __launch_bounds__(kIndexThreads)
   if constexpr (kTma) {
     if (tid == 0) {
       const uint32_t bar = smem_u32(&s_bar);
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile(
           "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
@@ -356,7 +362,10 @@ __global__ void __launch_bounds__(kIndexThreads)
   const uint32_t tp0 = trailing_escape_parity(c0.bs);
   const uint32_t tp1 = trailing_escape_parity(c1.bs);
   if (lane == 31) s_last_tp[warp] = tp1;
-  __syncthreads();  // (1) s_last_tp, s_halo
+  __syncthreads();  // (1) s_last_tp, s_halo; every thread is past the barrier wait
+  if constexpr (kTma) {
+    if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&s_bar)));
+  }
   uint32_t cin0 = __shfl_up_sync(0xFFFFFFFFu, tp1, 1);
   if (lane == 0) cin0 = (warp == 0) ? s_halo : s_last_tp[warp - 1];
 

@@ -47,8 +47,16 @@ METRIC = "index+query GB/s"
 L2_BYTES = 126 * 1024 * 1024
 
 
-def workload(name: str, pkg):
+def workload(name: str, pkg, size_mib: int | None = None):
     dg = pkg.datagen
+    if size_mib:
+        # profiling runs: the same generator and query at another size
+        sz = size_mib << 20
+        if name == "c1":
+            return (dg.products(1, sz), ["$[*].categoryPath[1:3].id"], "array",
+                    f"c1 generator at {size_mib} MiB, $[*].categoryPath[1:3].id")
+        return (dg.tweets(0, sz), ["$.user.lang"], "lines",
+                f"c0 generator at {size_mib} MiB, $.user.lang")
     if name == "c0":
         data = dg.tweets(0, 64 << 20)
         queries, records = ["$.user.lang"], "lines"
@@ -83,56 +91,56 @@ def compile_all(pkg, queries):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """Polls SM clocks and throttle reasons through NVML in a background
+    thread for the whole timed region (about one sample per millisecond)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[int, int]] = []
+        self.max_mhz = None
+        self.ok = False
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.device]) if vis else self.device
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.nv = pynvml
+            self.ok = True
+        except Exception:
+            self.ok = False
+            return
+        self.stop_flag = threading.Event()
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((mhz, rs))
+            except Exception:
+                pass
+            time.sleep(0.001)
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        self.stop_flag.set()
+        self.t.join()
+        reasons = sorted({k for _, rs in self.samples for k, bit in self.REASONS.items()
+                          if rs & bit})
+        mhz = [m for m, _ in self.samples]
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(mhz)}
 
 
 def measured_peak_hbm() -> tuple[float, str]:
@@ -187,7 +195,7 @@ def run_ours(args, world, rank, local):
     import torch
     pkg = entry.package()
     pkg.load_library()
-    data, queries, records, desc = workload(args.workload, pkg)
+    data, queries, records, desc = workload(args.workload, pkg, args.size_mib)
     comp = compile_all(pkg, queries)
     levels = max(c.max_depth + base for c, base in comp)
     n = int(data.size)
@@ -387,6 +395,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size-mib", type=int, default=None,
+                    help="profiling: run the workload's generator at this size")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_init()
