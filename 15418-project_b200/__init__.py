@@ -43,7 +43,8 @@ MAX_QUERY_DEPTH = 16
 
 EXPORTED_SYMBOLS = (
     "gpj_version", "gpj_last_error", "gpj_ctx_create", "gpj_ctx_destroy",
-    "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_free",
+    "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_build_noalloc",
+    "gpj_index_free",
     "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
 )
 
@@ -156,6 +157,7 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_compile.argtypes = [C.c_char_p, u64, vp, u64, P(u64), P(u64), P(u64)]
     lib.gpj_index_build.argtypes = [vp, vp, u64, i32, u32, P(Index), vp]
     lib.gpj_index_build_async.argtypes = [vp, vp, u64, i32, u32, P(Index), vp, vp]
+    lib.gpj_index_build_noalloc.argtypes = [vp, u64, i32, u32, P(Index), vp, vp]
     lib.gpj_index_free.argtypes = [vp, P(Index)]
     lib.gpj_query_run.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
     lib.gpj_query_run64.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
@@ -199,6 +201,19 @@ def compile(query: str, wildcard_limit: int = 0) -> CompiledQuery:  # noqa: A001
         _check(rc)
         break
     return CompiledQuery(query, bytes(buf[: n.value]), depth.value, slots.value)
+
+
+NOALLOC_MAX_BYTES = 4 << 30
+
+
+def build_index_noalloc(d_input: int, size_bytes: int, num_levels: int, index: Index,
+                        d_summary: int, flags: int = 0, stream: int = 0) -> None:
+    """gpj_index_build_noalloc: the index build for callers that cannot allocate
+    device memory (all buffers are the caller's; scratch is a fixed array in
+    the library, inputs up to 4 GiB)."""
+    _check(load_library().gpj_index_build_noalloc(
+        C.c_void_p(d_input), size_bytes, num_levels, flags, C.byref(index),
+        C.c_void_p(d_summary), C.c_void_p(stream)))
 
 
 class Context:

@@ -238,6 +238,11 @@ int run_query(gpj_ctx *ctx, const gpj_index *ix, const uint8_t *h_ir, uint64_t i
 
 }  // namespace
 
+namespace gpjb {
+// Records the last-error message for entry points defined in other files.
+int report_error(int code, const char *message) { return fail(code, message); }
+}  // namespace gpjb
+
 extern "C" {
 
 int gpj_version(void) { return 100; }

@@ -109,6 +109,24 @@ int gpj_index_build_async(gpj_ctx *ctx, const uint8_t *d_input,
                           uint64_t size_bytes, int num_levels, uint32_t flags,
                           gpj_index *index, uint64_t *d_summary, void *stream);
 
+/* Index build that allocates nothing, for callers that cannot call
+ * cudaMalloc: hosts that reserve all device memory up front and hand out
+ * pieces themselves (a database or serving engine that owns the GPU's memory
+ * pool), and latency-critical loops that avoid cudaMalloc/cudaFree because
+ * those calls can synchronize the device.  No counterpart in the reference.
+ * Same inputs, outputs and results as gpj_index_build_async (caller-owned
+ * index buffers and d_summary[0..3]: lines, in-string, depth, error bits);
+ * no context is needed.  Its scratch is a fixed 1 MiB device array inside the
+ * library, so size_bytes is limited to 4 GiB (GPJ_ERR_CAPACITY beyond).  The
+ * first call on a device looks up that array's device address (make it
+ * before any stream capture).  All calls on a device share the array: calls
+ * whose work overlaps on the GPU race.  Unaligned inputs use plain loads
+ * instead of TMA. */
+#define GPJ_NOALLOC_MAX_BYTES 4294967296ull
+int gpj_index_build_noalloc(const uint8_t *d_input, uint64_t size_bytes,
+                            int num_levels, uint32_t flags, gpj_index *index,
+                            uint64_t *d_summary, void *stream);
+
 /* Releases what gpj_index_build allocated. */
 int gpj_index_free(gpj_ctx *ctx, gpj_index *index);
 
