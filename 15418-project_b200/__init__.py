@@ -46,7 +46,13 @@ EXPORTED_SYMBOLS = (
     "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_build_noalloc",
     "gpj_index_free",
     "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
+    "gpj_batch_create", "gpj_batch_run", "gpj_batch_view_get", "gpj_batch_file_layout",
+    "gpj_batch_destroy",
 )
+
+GPJ_BATCH_AUTOTUNE = 4
+GPJ_BATCH_NO_GRAPH = 8
+FILE_INFO_WORDS = 8  # lines, newline slot, first record, first result int, in-string, depth, bytes, query
 
 
 # Exception hierarchy of the reference (include/gpjson/error/*.hpp).
@@ -125,6 +131,27 @@ class Index(C.Structure):
     ]
 
 
+class BatchFile(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("size_bytes", C.c_uint64), ("query", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class BatchQuery(C.Structure):
+    _fields_ = [("h_ir", C.c_void_p), ("ir_len", C.c_uint64), ("num_result_slots", C.c_uint32),
+                ("base_level", C.c_uint32), ("num_levels", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class BatchView(C.Structure):
+    _fields_ = [("d_string", C.c_void_p), ("d_leveled", C.c_void_p), ("d_newline", C.c_void_p),
+                ("d_results", C.c_void_p), ("d_file_info", C.c_void_p), ("d_totals", C.c_void_p),
+                ("num_files", C.c_uint64), ("num_records", C.c_uint64),
+                ("result_ints", C.c_uint64), ("newline_slots", C.c_uint64),
+                ("string_words", C.c_uint64), ("leveled_words", C.c_uint64),
+                ("num_tiles", C.c_uint32), ("index_threads", C.c_uint32),
+                ("query_block", C.c_uint32), ("query_grid", C.c_uint32),
+                ("uses_graph", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 _lib = None
 
 
@@ -163,6 +190,12 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_query_run64.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
     lib.gpj_query_run_opts.argtypes = [vp, P(Index), vp, u64, u32, P(QueryOpts), vp, vp]
     lib.gpj_query_host.argtypes = [vp, vp, u64, i32, u32, vp, vp, vp, vp, vp, vp, P(u64), vp]
+    lib.gpj_batch_create.argtypes = [vp, vp, u64, P(BatchFile), u32, P(BatchQuery), u32, u32,
+                                     P(vp), vp]
+    lib.gpj_batch_run.argtypes = [vp, vp]
+    lib.gpj_batch_view_get.argtypes = [vp, P(BatchView)]
+    lib.gpj_batch_file_layout.argtypes = [vp, u32, P(u64), P(u64), P(u32)]
+    lib.gpj_batch_destroy.argtypes = [vp]
     for name in EXPORTED_SYMBOLS:
         if name != "gpj_version" and name != "gpj_last_error":
             getattr(lib, name).restype = i32
@@ -297,3 +330,69 @@ class Context:
                                         q, ir_ptrs, ir_lens, slots, bases, outs, caps,
                                         C.byref(lines), C.c_void_p(stream)))
         return lines.value
+
+
+def pack_files(files, align: int = 128):
+    """Concatenates host byte arrays at `align`-byte offsets (zero padding).
+    Returns (buffer, offsets)."""
+    import numpy as np
+    offsets, pos = [], 0
+    for f in files:
+        offsets.append(pos)
+        pos += (len(f) + align - 1) // align * align
+    buf = np.zeros(max(pos, align), np.uint8)
+    for f, o in zip(files, offsets):
+        buf[o:o + len(f)] = np.frombuffer(bytes(f), np.uint8) if not hasattr(f, "dtype") else f
+    return buf, offsets
+
+
+class Batch:
+    """gpj_batch: many files indexed and queried by one captured launch chain.
+
+    files: list of (offset, size_bytes, query_index) in the device buffer;
+    queries: list of (CompiledQuery, base_level, num_levels)."""
+
+    def __init__(self, d_input: int, input_bytes: int, files, queries, flags: int = 0,
+                 stream: int = 0):
+        self._lib = load_library()
+        fa = (BatchFile * len(files))(*[BatchFile(o, n, q, 0) for o, n, q in files])
+        self._irs = [(C.c_uint8 * max(1, len(c.ir_bytes))).from_buffer_copy(c.ir_bytes or b"\0")
+                     for c, _, _ in queries]
+        qa = (BatchQuery * len(queries))(*[
+            BatchQuery(C.addressof(ir), len(c.ir_bytes), c.num_result_slots, base, lv, 0)
+            for (c, base, lv), ir in zip(queries, self._irs)])
+        h = C.c_void_p()
+        _check(self._lib.gpj_batch_create(None, C.c_void_p(d_input), input_bytes, fa, len(files),
+                                          qa, len(queries), flags, C.byref(h),
+                                          C.c_void_p(stream)))
+        self._h = h
+
+    def run(self, stream: int = 0) -> None:
+        _check(self._lib.gpj_batch_run(self._h, C.c_void_p(stream)))
+
+    def view(self) -> BatchView:
+        v = BatchView()
+        _check(self._lib.gpj_batch_view_get(self._h, C.byref(v)))
+        return v
+
+    def file_layout(self, f: int):
+        s, l, lv = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        _check(self._lib.gpj_batch_file_layout(self._h, f, C.byref(s), C.byref(l), C.byref(lv)))
+        return s.value, l.value, lv.value
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.gpj_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

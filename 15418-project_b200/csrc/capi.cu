@@ -79,8 +79,8 @@ uint64_t nl_capacity_guess(uint64_t n) { return n / 32u + 1024u; }
 int enqueue_index(gpj_ctx *ctx, const uint8_t *in, uint64_t n, int levels,
                   uint32_t flags, const gpj_index &out, cudaStream_t stream) {
   gpjb::IndexLaunch L;
-  L.n = n;
-  L.W = (n + 63u) / 64u;
+  L.single.n = n;
+  L.single.levels = levels;
   L.num_levels = levels;
   L.full_rows = n / 128u;
   L.S = out.d_string;

@@ -28,39 +28,56 @@ namespace {
 
 // ----------------------------------------------------------------------------
 // Look-back descriptor: one 64-bit word per tile, written with one store.
-//   bits 0-1  status (0 = not ready, 1 = aggregate, 2 = inclusive prefix)
-//   bit  2    string parity of the tile (quotes it toggles, mod 2)
-//   bits 3-10 depth change if the tile starts outside a string (mod 256)
+//   bits 0-1   status (0 = not ready, 1 = aggregate, 2 = inclusive prefix)
+//   bit  2     string parity: string state after the span if it starts
+//              outside a string (for a constant span: the state after it)
+//   bits 3-10  depth change if the span starts outside a string (mod 256)
 //   bits 11-18 depth change if it starts inside a string (mod 256)
-//   bits 19-63 newline count
-// An inclusive descriptor holds the prefix from the start of the partition,
-// evaluated for the initial state (outside a string, depth -1): its bit 2 is
-// the string state after the tile and bits 3-10 the depth sum.
+//   bit  19    constant: the span starts at a file start (state and depth
+//              restart there), so its result does not depend on what came
+//              before; inclusive prefixes are constant too
+//   bits 20-63 newline count (runs on across files)
+// A span is a function from the (string state, depth) entering it to the
+// pair leaving it; composition of such functions is associative, which is
+// what lets one warp fold 128 predecessors per step.
 // ----------------------------------------------------------------------------
 constexpr uint64_t kStatusAgg = 1, kStatusIncl = 2;
 
 struct Agg {
-  uint32_t p;   // string parity
+  uint32_t p;   // string parity (or final state for a constant span)
   uint32_t d0;  // depth change starting outside a string (mod 256)
   uint32_t d1;  // depth change starting inside a string (mod 256)
+  uint32_t c;   // 1 = constant span
   uint64_t n;   // newlines
 };
 
-__device__ __forceinline__ Agg agg_identity() { return Agg{0u, 0u, 0u, 0ull}; }
+__device__ __forceinline__ Agg agg_identity() { return Agg{0u, 0u, 0u, 0u, 0ull}; }
 
 // `a` covers the bytes before `b`.
 __device__ __forceinline__ Agg agg_combine(const Agg &a, const Agg &b) {
   Agg r;
-  r.p = a.p ^ b.p;
-  r.d0 = (a.d0 + (a.p ? b.d1 : b.d0)) & 0xFFu;
-  r.d1 = (a.d1 + (a.p ? b.d0 : b.d1)) & 0xFFu;
   r.n = a.n + b.n;
+  if (b.c) {  // b restarts: what came before only adds newlines
+    r.p = b.p;
+    r.d0 = b.d0;
+    r.d1 = b.d1;
+    r.c = 1u;
+  } else if (a.c) {  // constant a: b sees a's final state
+    r.p = a.p ^ b.p;
+    r.d0 = r.d1 = (a.d0 + (a.p ? b.d1 : b.d0)) & 0xFFu;
+    r.c = 1u;
+  } else {
+    r.p = a.p ^ b.p;
+    r.d0 = (a.d0 + (a.p ? b.d1 : b.d0)) & 0xFFu;
+    r.d1 = (a.d1 + (a.p ? b.d0 : b.d1)) & 0xFFu;
+    r.c = 0u;
+  }
   return r;
 }
 
 __device__ __forceinline__ uint64_t agg_pack(uint64_t status, const Agg &a) {
   return status | (uint64_t(a.p & 1u) << 2) | (uint64_t(a.d0 & 0xFFu) << 3) |
-         (uint64_t(a.d1 & 0xFFu) << 11) | (a.n << 19);
+         (uint64_t(a.d1 & 0xFFu) << 11) | (uint64_t(a.c & 1u) << 19) | (a.n << 20);
 }
 
 __device__ __forceinline__ Agg agg_unpack(uint64_t v) {
@@ -68,12 +85,14 @@ __device__ __forceinline__ Agg agg_unpack(uint64_t v) {
   a.p = uint32_t(v >> 2) & 1u;
   a.d0 = uint32_t(v >> 3) & 0xFFu;
   a.d1 = uint32_t(v >> 11) & 0xFFu;
-  a.n = v >> 19;
+  a.c = uint32_t(v >> 19) & 1u;
+  a.n = v >> 20;
   return a;
 }
 
 __device__ __forceinline__ Agg shfl_down_agg(const Agg &a, int off) {
   Agg r;
+  r.c = __shfl_down_sync(0xFFFFFFFFu, a.c, off);
   r.p = __shfl_down_sync(0xFFFFFFFFu, a.p, off);
   r.d0 = __shfl_down_sync(0xFFFFFFFFu, a.d0, off);
   r.d1 = __shfl_down_sync(0xFFFFFFFFu, a.d1, off);
@@ -95,46 +114,68 @@ __device__ __forceinline__ void st_relaxed(unsigned long long *p, uint64_t v) {
 // invariant surfaces as an error status on the host instead of a hang.
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-// Warp 0 only.  Publishes the tile's aggregate, walks back over predecessors
-// 32 at a time and returns the exclusive prefix of the tile.
+// Warp 0 only.  Publishes the tile's aggregate, then walks back over its
+// predecessors, 128 per round (4 consecutive descriptors per lane, loaded
+// together so one round costs one memory round trip), and returns the tile's
+// exclusive prefix.
+constexpr int kLookbackPerLane = 4;
+
 __device__ Agg lookback(const IndexLaunch &P, uint32_t tile, const Agg &local) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) return agg_identity();
   if (lane == 0) st_relaxed(&P.tile_state[tile], agg_pack(kStatusAgg, local));
 
   Agg later = agg_identity();
-  int64_t base = int64_t(tile) - 1;
+  int64_t base = int64_t(tile) - 1;  // newest tile of the window
   for (;;) {
-    const int64_t idx = base - lane;
-    uint64_t s = 0;
+    // lane l covers tiles base - 4l - j, j = 0 (newest) .. 3 (oldest)
+    uint64_t s[kLookbackPerLane];
     uint32_t polls = 0;
     for (;;) {
-      s = (idx >= 0) ? ld_relaxed(&P.tile_state[idx]) : kStatusIncl;
-      const bool ready = (s & 3u) != 0;
+      bool ready = true;
+#pragma unroll
+      for (int j = 0; j < kLookbackPerLane; ++j) {
+        const int64_t idx = base - int64_t(kLookbackPerLane) * lane - j;
+        s[j] = (idx >= 0) ? ld_relaxed(&P.tile_state[idx]) : kStatusIncl;
+        ready = ready && ((s[j] & 3u) != 0);
+      }
       if (__all_sync(0xFFFFFFFFu, ready)) break;
       if (++polls > kSpinLimit) {
         if (lane == 0) atomicOr(P.error, kErrLookbackTimeout);
-        if (!ready) s = kStatusIncl;
+#pragma unroll
+        for (int j = 0; j < kLookbackPerLane; ++j)
+          if ((s[j] & 3u) == 0) s[j] = kStatusIncl;
         break;
       }
       __nanosleep(polls < 64 ? 20 : 500);
     }
-    const uint32_t incl = __ballot_sync(0xFFFFFFFFu, (s & 3u) == kStatusIncl);
+    // fold the lane's descriptors newest-first, stopping at an inclusive one
+    Agg v = agg_identity();
+    bool has_incl = false;
+#pragma unroll
+    for (int j = 0; j < kLookbackPerLane; ++j) {
+      if (!has_incl) {
+        v = agg_combine(agg_unpack(s[j]), v);
+        has_incl = (s[j] & 3u) == kStatusIncl;
+      }
+    }
+    const uint32_t incl = __ballot_sync(0xFFFFFFFFu, has_incl);
     const int limit = incl ? (__ffs(incl) - 1) : 31;
-    Agg v = (lane <= limit) ? agg_unpack(s) : agg_identity();
+    if (lane > limit) v = agg_identity();
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const Agg o = shfl_down_agg(v, off);  // tiles further back
       if (lane + off < 32) v = agg_combine(o, v);
     }
     Agg window;
+    window.c = __shfl_sync(0xFFFFFFFFu, v.c, 0);
     window.p = __shfl_sync(0xFFFFFFFFu, v.p, 0);
     window.d0 = __shfl_sync(0xFFFFFFFFu, v.d0, 0);
     window.d1 = __shfl_sync(0xFFFFFFFFu, v.d1, 0);
     window.n = __shfl_sync(0xFFFFFFFFu, v.n, 0);
     later = agg_combine(window, later);
     if (incl) break;
-    base -= 32;
+    base -= 32 * kLookbackPerLane;
   }
   return later;
 }
@@ -145,44 +186,33 @@ __device__ Agg lookback(const IndexLaunch &P, uint32_t tile, const Agg &local) {
 // signed char, as in sharemem/leveled-bitmaps-index.cu:270-300.
 // ----------------------------------------------------------------------------
 template <int LMAX>
-__device__ __forceinline__ void add_level(uint64_t (&lb)[LMAX], int d,
-                                          uint64_t m, int L) {
-  if (m == 0 || d < 0 || d >= L) return;
+__device__ __forceinline__ void add_level(uint64_t (&lb)[LMAX], int d, uint64_t m) {
+  // levels >= L are computed but never stored; d outside [0, LMAX) matches none
 #pragma unroll
-  for (int l = 0; l < LMAX; ++l)
-    if (d == l) lb[l] |= m;
+  for (int l = 0; l < LMAX; ++l) lb[l] |= (d == l) ? m : 0ull;
 }
 
 template <int LMAX>
 __device__ __forceinline__ int leveled_word(uint64_t op, uint64_t cl,
-                                            uint64_t sp, int depth, int L,
+                                            uint64_t sp, int depth,
                                             uint64_t (&lb)[LMAX]) {
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) lb[l] = 0;
   uint64_t ev = op | cl;
-  if (ev == 0) {
-    add_level<LMAX>(lb, depth, sp, L);
-    return depth;
-  }
   int d = depth;
   uint64_t acc = 0, done = 0;
-  while (ev) {
+  while (ev) {  // branch-free body: lanes only differ in the trip count
     const uint64_t bit = ev & (0 - ev);
     const uint64_t below = bit - 1;
     acc |= sp & below & ~done;
-    if (op & bit) {
-      add_level<LMAX>(lb, d, acc, L);
-      d = int(int8_t(d + 1));
-      acc = bit;
-    } else {
-      add_level<LMAX>(lb, d, acc | bit, L);
-      d = int(int8_t(d - 1));
-      acc = 0;
-    }
+    const bool open = (op & bit) != 0;
+    add_level<LMAX>(lb, d, open ? acc : (acc | bit));
+    d = int(int8_t(open ? d + 1 : d - 1));
+    acc = open ? bit : 0ull;
     done = below | bit;
     ev &= ev - 1;
   }
-  add_level<LMAX>(lb, d, acc | (sp & ~done), L);
+  add_level<LMAX>(lb, d, acc | (sp & ~done));
   return d;
 }
 
@@ -208,7 +238,7 @@ __device__ __forceinline__ void store2(uint64_t *dst, uint64_t w, uint64_t W,
   }
 }
 
-// Loads 64 bytes [base, base+64) of the input as 16 registers, zero past n.
+// Loads 64 bytes [base, base+64) of `in` as 16 registers, zero at and past n.
 __device__ __forceinline__ void load_word_global(const uint8_t *in, uint64_t n,
                                                  uint64_t base, uint32_t (&r)[16]) {
   if (base + 64u <= n && (reinterpret_cast<uintptr_t>(in + base) & 15u) == 0) {
@@ -255,17 +285,34 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-template <int LMAX, bool kTma>
-__global__ void __launch_bounds__(kIndexThreads)
+// Locates the file of `tile`: binary search over the files' first tiles.
+__device__ __forceinline__ uint32_t file_of_tile(const IndexLaunch &P, uint32_t tile) {
+  uint32_t lo = 0, hi = P.num_files;  // invariant: files[lo].first_tile <= tile
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (P.files[mid].first_tile <= tile) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// NT threads per CTA, two 64-byte words per thread: a tile is NT * 128 bytes
+// (NT rows of 128 B, one TMA box).
+template <int LMAX, bool kTma, int NT>
+__global__ void __launch_bounds__(NT)
     index_kernel(const __grid_constant__ CUtensorMap tmap, const IndexLaunch P) {
-  __shared__ __align__(1024) uint8_t s_tile[kTma ? kTileBytes : 16];
+  constexpr int NWARPS = NT / 32;
+  constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
+  static_assert(NT % 32 == 0 && NT <= 256, "one TMA box of at most 256 rows per tile");
+  __shared__ __align__(1024) uint8_t s_tile[kTma ? TILE_BYTES : 16];
   __shared__ __align__(8) uint64_t s_bar;
-  __shared__ uint32_t s_tile_id;
+  __shared__ uint32_t s_tile_id, s_file_idx;
+  __shared__ IndexFile s_file;
   __shared__ uint32_t s_halo;
-  __shared__ uint32_t s_last_tp[8];
-  __shared__ uint32_t s_warp_par[8];
-  __shared__ uint32_t s_warp_dd[8];
-  __shared__ uint32_t s_warp_nl[8];
+  __shared__ uint32_t s_last_tp[NWARPS];
+  __shared__ uint32_t s_warp_par[NWARPS];
+  __shared__ uint32_t s_warp_dd[NWARPS];
+  __shared__ uint32_t s_warp_nl[NWARPS];
   __shared__ uint32_t s_prefix_p, s_prefix_d;
   __shared__ unsigned long long s_prefix_n;
 
@@ -274,7 +321,16 @@ __global__ void __launch_bounds__(kIndexThreads)
   const int warp = tid >> 5;
 
   if (tid == 0) {
-    s_tile_id = atomicAdd(P.tile_counter, 1u);
+    const uint32_t t = atomicAdd(P.tile_counter, 1u);
+    s_tile_id = t;
+    if (P.files == nullptr) {
+      s_file_idx = 0;
+      s_file = P.single;
+    } else if (t < P.num_tiles) {
+      const uint32_t f = file_of_tile(P, t);
+      s_file_idx = f;
+      s_file = P.files[f];
+    }
     if constexpr (kTma) {
       // the barrier must be initialised before any thread polls it: shared
       // memory may still hold a barrier of an earlier CTA on this SM
@@ -285,9 +341,15 @@ __global__ void __launch_bounds__(kIndexThreads)
   __syncthreads();
   const uint32_t tile = s_tile_id;
   if (tile >= P.num_tiles) return;  // cannot happen with grid == num_tiles
-  const uint64_t tile_byte0 = uint64_t(tile) * kTileBytes;
-  const uint64_t tile_word0 = uint64_t(tile) * kTileWords;
-  const int64_t row0 = int64_t(tile) * kTileRows;
+  const IndexFile F = s_file;
+  const uint32_t file_idx = s_file_idx;
+  const uint32_t ktile = tile - F.first_tile;             // tile within the file
+  const bool file_start = ktile == 0;
+  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;    // tile start within the file
+  const uint64_t valid = min(TILE_BYTES, F.n - byte0);    // bytes of the file in the tile
+  const uint64_t W = (F.n + 63u) / 64u;                   // words of the file
+  const uint8_t *fin = P.in + F.in_off;                   // file bytes
+  const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
 
   if constexpr (kTma) {
     if (tid == 0) {
@@ -295,7 +357,7 @@ __global__ void __launch_bounds__(kIndexThreads)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile(
           "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-          "r"(uint32_t(kTileBytes))
+          "r"(uint32_t(TILE_BYTES))
           : "memory");
       asm volatile(
           "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
@@ -305,56 +367,54 @@ __global__ void __launch_bounds__(kIndexThreads)
     }
   }
   // Escape carry into the tile: parity of the backslash run that ends the
-  // previous word (read backward, at most 64 bytes).
+  // previous word of the same file (read backward, at most 64 bytes).
   if (tid == 0) {
     uint32_t p = 0;
-    if (tile > 0) {
+    if (!file_start) {
       for (int k = 1; k <= 64; ++k) {
-        if (P.in[tile_byte0 - uint64_t(k)] == '\\') p ^= 1u;
+        if (fin[byte0 - uint64_t(k)] == '\\') p ^= 1u;
         else break;
       }
     }
     s_halo = p;
   }
 
-  const int64_t my_row = row0 + tid;
-  const uint64_t w0 = tile_word0 + 2u * uint64_t(tid);  // my first word
-  uint32_t r[16];
-  WordClasses c0, c1;
+  // Thread `tid` owns tile row `tid`: bytes [128 tid, 128 tid + 128) of the
+  // tile, i.e. words lw0 and lw0 + 1 of the file.
+  const uint64_t row_byte = uint64_t(tid) * 128u;
+  const uint64_t lw0 = byte0 / 64u + 2u * uint64_t(tid);
+  const bool row_in_smem = kTma && row_byte + 128u <= valid &&
+                           row0 + tid < int64_t(P.full_rows);
   if constexpr (kTma) {
-    if (my_row >= int64_t(P.full_rows)) {
-      load_word_global(P.in, P.n, w0 * 64u, r);
-      c0 = classify64(r);
-      load_word_global(P.in, P.n, w0 * 64u + 64u, r);
-      c1 = classify64(r);
-      // still take part in the barrier wait below via the shared path
-    }
-    {
-      const uint32_t bar = smem_u32(&s_bar);
-      uint32_t done = 0, polls = 0;
-      while (!done) {
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;"
-            " selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
-        if (!done && ++polls > kSpinLimit) {
-          atomicOr(P.error, kErrTmaTimeout);
-          break;
-        }
+    const uint32_t bar = smem_u32(&s_bar);
+    uint32_t done = 0, polls = 0;
+    while (!done) {
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;"
+          " selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+      if (!done && ++polls > kSpinLimit) {
+        atomicOr(P.error, kErrTmaTimeout);
+        break;
       }
     }
-    if (my_row < int64_t(P.full_rows)) {
-      load_word_smem(s_tile, tid, 0, r);
-      c0 = classify64(r);
-      load_word_smem(s_tile, tid, 1, r);
-      c1 = classify64(r);
-    }
-  } else {
-    load_word_global(P.in, P.n, w0 * 64u, r);
+  }
+  uint32_t r[16];
+  WordClasses c0, c1;
+  if (row_in_smem) {
+    load_word_smem(s_tile, tid, 0, r);
     c0 = classify64(r);
-    load_word_global(P.in, P.n, w0 * 64u + 64u, r);
+    load_word_smem(s_tile, tid, 1, r);
+    c1 = classify64(r);
+  } else {
+    // rows past the end of the file read as zero bytes (no class)
+    const uint64_t lim = valid > row_byte ? valid - row_byte : 0u;
+    const uint8_t *rp = fin + byte0 + row_byte;
+    load_word_global(rp, lim, 0, r);
+    c0 = classify64(r);
+    load_word_global(rp, lim, 64, r);
     c1 = classify64(r);
   }
 
@@ -397,10 +457,10 @@ __global__ void __launch_bounds__(kIndexThreads)
   for (int w = 0; w < warp; ++w) pex ^= s_warp_par[w];
   uint32_t tile_par = 0;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) tile_par ^= s_warp_par[w];
+  for (int w = 0; w < NWARPS; ++w) tile_par ^= s_warp_par[w];
 
   // depth changes are only needed mod 256: two 16-bit lanes cannot overflow
-  // over 256 threads (256 * 255 < 65536)
+  // over at most 256 threads (256 * 255 < 65536)
   const int dt0 = pex ? (thr_t - thr_d0) : thr_d0;
   uint32_t dd = (uint32_t(dt0) & 0xFFu) | ((uint32_t(thr_t) & 0xFFu) << 16);
   uint32_t nl = thr_nl;
@@ -422,7 +482,7 @@ __global__ void __launch_bounds__(kIndexThreads)
   uint32_t dd_ex = dd_inc - dd, nl_ex = nl_inc - nl;
   uint32_t tile_dd = 0, tile_nl = 0;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) {
+  for (int w = 0; w < NWARPS; ++w) {
     if (w < warp) {
       dd_ex += s_warp_dd[w];
       nl_ex += s_warp_nl[w];
@@ -437,26 +497,30 @@ __global__ void __launch_bounds__(kIndexThreads)
     local.p = tile_par;
     local.d0 = tile_dd & 0xFFu;
     local.d1 = ((tile_dd >> 16) - tile_dd) & 0xFFu;  // total - d0
+    local.c = file_start ? 1u : 0u;
+    if (file_start) local.d1 = local.d0;  // a file starts outside any string
     local.n = tile_nl;
     const Agg prefix = lookback(P, tile, local);
     if (lane == 0) {
       const Agg incl = agg_combine(prefix, local);
       st_relaxed(&P.tile_state[tile], agg_pack(kStatusIncl, incl));
-      s_prefix_p = prefix.p;
-      s_prefix_d = prefix.d0;
+      // a file start ignores the string state and depth of what precedes it
+      s_prefix_p = file_start ? 0u : prefix.p;
+      s_prefix_d = file_start ? 0u : prefix.d0;
       s_prefix_n = prefix.n;
-      if (tile + 1 == P.num_tiles) {
+      if (P.files == nullptr && tile + 1 == P.num_tiles) {
         P.summary[0] = incl.n + 1u;  // lines = newlines + 1
         P.summary[1] = incl.p;
         P.summary[2] = uint64_t(int64_t(int8_t(uint8_t(incl.d0 - 1u))));
       }
-      if (tile == 0 && P.nl_cap > 0) P.NL[0] = 0;
+      // newline index of the file starts with 0, at (newlines before it) + f
+      if (file_start && prefix.n + file_idx < P.nl_cap) P.NL[prefix.n + file_idx] = 0;
     }
   }
   __syncthreads();  // (4)
   const uint32_t c_in = s_prefix_p;
   const uint32_t d_in = s_prefix_d;
-  const uint64_t nl_base = s_prefix_n + nl_ex;
+  const uint64_t nl_base = s_prefix_n + nl_ex + file_idx;  // slot of my first newline - 1
 
   // --- outputs ----------------------------------------------------------------
   const uint32_t car0 = c_in ^ pex;
@@ -466,53 +530,62 @@ __global__ void __launch_bounds__(kIndexThreads)
   const uint32_t a_ex = dd_ex & 0xFFu, t_ex = (dd_ex >> 16) & 0xFFu;
   const int depth0 = int(int8_t(uint8_t(d_in - 1u + (c_in ? (t_ex - a_ex) : a_ex))));
 
-  store2(P.S, w0, P.W, S0, S1);
+  store2(P.S + F.s_off, lw0, W, S0, S1);
   if (P.E != nullptr) {
-    store2(P.E, w0, P.W, E0 & valid_mask(w0, P.n), E1 & valid_mask(w0 + 1, P.n));
-    store2(P.Q, w0, P.W, Q0, Q1);
+    store2(P.E + F.s_off, lw0, W, E0 & valid_mask(lw0, F.n), E1 & valid_mask(lw0 + 1, F.n));
+    store2(P.Q + F.s_off, lw0, W, Q0, Q1);
   }
 
-  if (P.num_levels > 0) {
+  if (F.levels > 0) {
     uint64_t lb0[LMAX], lb1[LMAX];
-    const int depth1 = leveled_word<LMAX>(c0.op & ~S0, c0.cl & ~S0, c0.sp & ~S0,
-                                          depth0, P.num_levels, lb0);
-    leveled_word<LMAX>(c1.op & ~S1, c1.cl & ~S1, c1.sp & ~S1, depth1,
-                       P.num_levels, lb1);
+    const int depth1 =
+        leveled_word<LMAX>(c0.op & ~S0, c0.cl & ~S0, c0.sp & ~S0, depth0, lb0);
+    leveled_word<LMAX>(c1.op & ~S1, c1.cl & ~S1, c1.sp & ~S1, depth1, lb1);
 #pragma unroll
     for (int l = 0; l < LMAX; ++l) {
-      if (l < P.num_levels) store2(P.LB + uint64_t(l) * P.W, w0, P.W, lb0[l], lb1[l]);
+      if (l < F.levels) store2(P.LB + F.lb_off + uint64_t(l) * W, lw0, W, lb0[l], lb1[l]);
     }
   }
 
-  // newline offsets (every '\n' counts, strings or not)
+  // newline offsets (every '\n' counts, strings or not), file-local
   uint64_t k = nl_base;
   uint64_t m = c0.nl;
   while (m) {
     const int b = __ffsll(static_cast<long long>(m)) - 1;
-    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t(w0 * 64u + uint64_t(b));
+    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t(lw0 * 64u + uint64_t(b));
     ++k;
     m &= m - 1;
   }
   m = c1.nl;
   while (m) {
     const int b = __ffsll(static_cast<long long>(m)) - 1;
-    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t((w0 + 1) * 64u + uint64_t(b));
+    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t((lw0 + 1) * 64u + uint64_t(b));
     ++k;
     m &= m - 1;
   }
 }
 
-template <int LMAX>
-cudaError_t launch_levels(const IndexLaunch &L, const CUtensorMap *map,
-                          bool use_tma, cudaStream_t stream) {
-  const dim3 grid(L.num_tiles), block(kIndexThreads);
+template <int LMAX, int NT>
+cudaError_t launch_levels(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
+                          cudaStream_t stream) {
+  const dim3 grid(L.num_tiles), block(NT);
   if (use_tma) {
-    index_kernel<LMAX, true><<<grid, block, 0, stream>>>(*map, L);
+    index_kernel<LMAX, true, NT><<<grid, block, 0, stream>>>(*map, L);
   } else {
     CUtensorMap dummy{};
-    index_kernel<LMAX, false><<<grid, block, 0, stream>>>(dummy, L);
+    index_kernel<LMAX, false, NT><<<grid, block, 0, stream>>>(dummy, L);
   }
   return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t launch_threads(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
+                           cudaStream_t stream) {
+  const int lv = L.num_levels;
+  if (lv <= 2) return launch_levels<2, NT>(L, map, use_tma, stream);
+  if (lv <= 4) return launch_levels<4, NT>(L, map, use_tma, stream);
+  if (lv <= 8) return launch_levels<8, NT>(L, map, use_tma, stream);
+  return launch_levels<kMaxLevels, NT>(L, map, use_tma, stream);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -540,14 +613,14 @@ void index_bind_scratch(IndexLaunch &L, void *scratch) {
   L.error = reinterpret_cast<unsigned int *>(tail + 36);
 }
 
-bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n) {
+bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n, int threads) {
   const uint64_t rows = n / 128u;
   if (rows == 0 || (reinterpret_cast<uintptr_t>(in) & 15u) != 0) return false;
   auto fn = encode_fn();
   if (fn == nullptr) return false;
   const cuuint64_t dims[2] = {128u, rows};
   const cuuint64_t strides[1] = {128u};
-  const cuuint32_t box[2] = {128u, uint32_t(kTileRows)};
+  const cuuint32_t box[2] = {128u, uint32_t(threads)};
   const cuuint32_t estr[2] = {1u, 1u};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
                         const_cast<uint8_t *>(in), dims, strides, box, estr,
@@ -557,17 +630,114 @@ bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n) {
   return r == CUDA_SUCCESS;
 }
 
-cudaError_t index_launch(const IndexLaunch &L, const CUtensorMap *map,
-                         bool use_tma, cudaStream_t stream) {
+cudaError_t index_launch(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
+                         cudaStream_t stream, int threads) {
   if (L.num_tiles == 0) return cudaSuccess;
   const uint64_t scratch = uint64_t(L.num_tiles) * 8u + 64u;
   cudaError_t e = cudaMemsetAsync(L.tile_state, 0, scratch, stream);
   if (e != cudaSuccess) return e;
-  const int lv = L.num_levels;
-  if (lv <= 2) return launch_levels<2>(L, map, use_tma, stream);
-  if (lv <= 4) return launch_levels<4>(L, map, use_tma, stream);
-  if (lv <= 8) return launch_levels<8>(L, map, use_tma, stream);
-  return launch_levels<kMaxLevels>(L, map, use_tma, stream);
+  if (threads == 128) return launch_threads<128>(L, map, use_tma, stream);
+  return launch_threads<256>(L, map, use_tma, stream);
+}
+}  // namespace gpjb
+
+namespace gpjb {
+namespace {
+
+constexpr int kFinalizeThreads = 1024;
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    finalize_files_kernel(const IndexLaunch P, const uint32_t *query_of_file,
+                          const uint32_t *slots_of_query, uint64_t *info, uint64_t *totals) {
+  __shared__ unsigned long long s_warp_rec[32], s_warp_out[32];
+  __shared__ unsigned long long s_carry_rec, s_carry_out;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    s_carry_rec = 0;
+    s_carry_out = 0;
+  }
+  __syncthreads();
+  for (uint32_t base = 0; base < P.num_files; base += kFinalizeThreads) {
+    const uint32_t f = base + uint32_t(tid);
+    uint64_t lines = 0, nl_off = 0, out_ints = 0, in_string = 0, bytes = 0;
+    int64_t depth = -1;
+    uint32_t q = 0;
+    if (f < P.num_files) {
+      const IndexFile F = P.files[f];
+      const uint32_t next_first = (f + 1 < P.num_files) ? P.files[f + 1].first_tile : P.num_tiles;
+      // newlines before the file = inclusive count of the tile before it
+      const uint64_t n_start = F.first_tile > 0 ? agg_unpack(P.tile_state[F.first_tile - 1]).n : 0;
+      const uint64_t n_end = next_first > 0 ? agg_unpack(P.tile_state[next_first - 1]).n : 0;
+      lines = n_end - n_start + 1u;
+      nl_off = n_start + f;
+      bytes = F.n;
+      if (next_first > F.first_tile) {
+        const Agg last = agg_unpack(P.tile_state[next_first - 1]);
+        in_string = last.p;
+        depth = int64_t(int8_t(uint8_t(last.d0 - 1u)));
+      } else if (nl_off < P.nl_cap) {
+        P.NL[nl_off] = 0;  // an empty file has no tile to write it
+      }
+      q = query_of_file ? query_of_file[f] : 0u;
+      out_ints = lines * uint64_t(slots_of_query ? slots_of_query[q] : 0u) * 2u;
+    }
+    // block-wide exclusive scans of lines and result ints
+    unsigned long long rec_inc = lines, out_inc = out_ints;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned long long a = __shfl_up_sync(0xFFFFFFFFu, rec_inc, off);
+      const unsigned long long b = __shfl_up_sync(0xFFFFFFFFu, out_inc, off);
+      if (lane >= off) {
+        rec_inc += a;
+        out_inc += b;
+      }
+    }
+    if (lane == 31) {
+      s_warp_rec[warp] = rec_inc;
+      s_warp_out[warp] = out_inc;
+    }
+    __syncthreads();
+    unsigned long long rec_ex = rec_inc - lines + s_carry_rec;
+    unsigned long long out_ex = out_inc - out_ints + s_carry_out;
+    for (int w = 0; w < warp; ++w) {
+      rec_ex += s_warp_rec[w];
+      out_ex += s_warp_out[w];
+    }
+    if (f < P.num_files) {
+      uint64_t *row = info + uint64_t(f) * kFileInfoWords;
+      row[kFiLines] = lines;
+      row[kFiNlOff] = nl_off;
+      row[kFiRecOff] = rec_ex;
+      row[kFiOutOff] = out_ex;
+      row[kFiInString] = in_string;
+      row[kFiDepth] = uint64_t(depth);
+      row[kFiBytes] = bytes;
+      row[kFiQuery] = q;
+    }
+    __syncthreads();
+    if (tid == kFinalizeThreads - 1) {
+      s_carry_rec = rec_ex + lines;
+      s_carry_out = out_ex + out_ints;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const uint64_t n_total = P.num_tiles > 0 ? agg_unpack(P.tile_state[P.num_tiles - 1]).n : 0;
+    totals[kTotRecords] = s_carry_rec;
+    totals[kTotResultInts] = s_carry_out;
+    totals[kTotNlSlots] = n_total + P.num_files;
+    totals[kTotError] = *P.error;
+  }
+}
+
+}  // namespace
+
+cudaError_t index_finalize_files(const IndexLaunch &L, const uint32_t *query_of_file,
+                                 const uint32_t *slots_of_query, uint64_t *file_info,
+                                 uint64_t *totals, cudaStream_t stream) {
+  finalize_files_kernel<<<1, kFinalizeThreads, 0, stream>>>(L, query_of_file, slots_of_query,
+                                                             file_info, totals);
+  return cudaGetLastError();
 }
 
 }  // namespace gpjb

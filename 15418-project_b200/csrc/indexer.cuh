@@ -15,21 +15,36 @@ constexpr uint64_t kTileBytes = uint64_t(kTileWords) * 64u;       // 32 KiB
 constexpr int kTileRows = int(kTileBytes / 128u);                 // 256 rows of 128 B
 constexpr int kMaxLevels = 22;  // kMaxNumLevels, sharemem/leveled-bitmaps-index.cu
 
+// One file (partition) of an indexed buffer.  Offsets are relative to the
+// IndexLaunch pointers.  Tiles never cross files; string state and depth
+// restart at each file, newline counting runs on across files so that every
+// file's newline index lands in one packed array.
+struct IndexFile {
+  uint64_t in_off = 0;     // byte offset in `in` (a multiple of 128 when TMA loads it)
+  uint64_t n = 0;          // bytes
+  uint64_t s_off = 0;      // first word of its S (and E, Q) words
+  uint64_t lb_off = 0;     // first word of its L * W leveled words (level-major)
+  uint32_t first_tile = 0; // index of its first tile
+  int32_t levels = 0;      // L of this file
+};
+
 // Everything one launch of the indexer reads and writes.  Device pointers.
 struct IndexLaunch {
-  const uint8_t *in = nullptr;  // partition bytes
-  uint64_t n = 0;               // partition size
-  uint64_t W = 0;               // ceil(n / 64)
-  int num_levels = 0;           // L, 0..kMaxLevels
-  uint64_t full_rows = 0;       // n / 128: rows the TMA descriptor covers
-  uint64_t *S = nullptr;        // [W]   string mask
-  uint64_t *LB = nullptr;       // [L*W] leveled bitmaps, level-major
-  uint64_t *E = nullptr;        // [W]   escape bitmap (verify mode) or null
-  uint64_t *Q = nullptr;        // [W]   quote bitmap (verify mode) or null
-  int64_t *NL = nullptr;        // newline index, nl_cap entries
+  const uint8_t *in = nullptr;  // input bytes
+  uint64_t full_rows = 0;       // whole 128-byte rows of `in` the TMA descriptor covers
+  IndexFile single;             // the file when `files` is null (one partition)
+  const IndexFile *files = nullptr;  // device table, num_files entries, or null
+  uint32_t num_files = 1;
+  int num_levels = 0;           // max L over the files (selects the kernel)
+  uint64_t *S = nullptr;        // string mask words
+  uint64_t *LB = nullptr;       // leveled bitmaps
+  uint64_t *E = nullptr;        // escape bitmap words (verify mode) or null
+  uint64_t *Q = nullptr;        // quote bitmap words (verify mode) or null
+  int64_t *NL = nullptr;        // newline indexes of all files, packed: file f
+                                // starts at (newlines before f) + f
   uint64_t nl_cap = 0;
   // scratch: one 64-bit look-back descriptor per tile, a tile ticket counter,
-  // an error word and a 4-word summary
+  // an error word and a 4-word summary (one-file launches)
   unsigned long long *tile_state = nullptr;
   unsigned int *tile_counter = nullptr;
   unsigned int *error = nullptr;
@@ -59,12 +74,50 @@ inline uint64_t index_scratch_bytes(uint64_t n) {
 void index_bind_scratch(IndexLaunch &L, void *scratch);
 
 // Encodes the TMA descriptor for `in` (2-D view: rows of 128 B, 128-byte
-// swizzle).  Returns false when the TMA path cannot be used (n < 128 or the
-// pointer is not 16-byte aligned); the launcher then uses plain loads.
-bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n);
+// swizzle, boxes of `threads` rows = one tile).  Returns false when the TMA
+// path cannot be used (n < 128 or the pointer is not 16-byte aligned); the
+// launcher then uses plain loads.
+bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n,
+                           int threads = kIndexThreads);
 
-// Zeroes the scratch and launches the indexer on `stream`.  No host sync.
+// Zeroes the scratch and launches the indexer on `stream` with `threads`
+// (128 or 256) threads per CTA: tiles of threads * 128 bytes, so num_tiles
+// and the files' first tiles must be counted with that tile size.
 cudaError_t index_launch(const IndexLaunch &L, const CUtensorMap *map,
-                         bool use_tma, cudaStream_t stream);
+                         bool use_tma, cudaStream_t stream,
+                         int threads = kIndexThreads);
+
+inline uint64_t tiles_for(uint64_t n, int threads) {
+  const uint64_t tb = uint64_t(threads) * 128u;
+  return (n + tb - 1) / tb;
+}
+
+}  // namespace gpjb
+
+namespace gpjb {
+
+// Per-file results of a multi-file index build (one row of 8 words per file).
+enum FileInfoField : int {
+  kFiLines = 0,     // newline count + 1
+  kFiNlOff = 1,     // first slot of its newline index in the packed array
+  kFiRecOff = 2,    // first record of the file in the batch record numbering
+  kFiOutOff = 3,    // first int of its result block
+  kFiInString = 4,  // string state after its last byte
+  kFiDepth = 5,     // signed-char depth after its last byte (as int64)
+  kFiBytes = 6,     // file size
+  kFiQuery = 7,     // query group
+  kFileInfoWords = 8,
+};
+
+// Totals of a multi-file build: [records, result ints, newline slots, error].
+enum TotalField : int { kTotRecords = 0, kTotResultInts = 1, kTotNlSlots = 2, kTotError = 3 };
+
+// After index_launch on a file table: derives every file's line count,
+// newline-index slot, record and result offsets (exclusive scans over the
+// files) from the tiles' inclusive look-back descriptors, writes the leading
+// 0 of each empty file's newline index, and the totals.  One CTA.
+cudaError_t index_finalize_files(const IndexLaunch &L, const uint32_t *query_of_file,
+                                 const uint32_t *slots_of_query, uint64_t *file_info,
+                                 uint64_t *totals, cudaStream_t stream);
 
 }  // namespace gpjb

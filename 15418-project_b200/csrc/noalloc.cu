@@ -119,8 +119,8 @@ extern "C" int gpj_index_build_noalloc(const uint8_t *d_input, uint64_t size_byt
   }
 
   gpjb::IndexLaunch L;
-  L.n = size_bytes;
-  L.W = W;
+  L.single.n = size_bytes;
+  L.single.levels = num_levels;
   L.num_levels = num_levels;
   L.full_rows = size_bytes / 128u;
   L.S = index->d_string;

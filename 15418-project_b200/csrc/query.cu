@@ -335,7 +335,44 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+__global__ void __launch_bounds__(256)
+    batch_query_kernel(const BatchQueryLaunch q, const __grid_constant__ IrBlob ir) {
+  __shared__ uint8_t s_ir[kMaxQueryIrBytes];
+  for (int i = threadIdx.x; i < kMaxQueryIrBytes; i += blockDim.x) s_ir[i] = ir.bytes[i];
+  __syncthreads();
+  const uint64_t records = q.totals[kTotRecords];
+  const uint64_t stride = uint64_t(blockDim.x) * gridDim.x;
+  for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < records; r += stride) {
+    uint32_t lo = 0, hi = q.num_files;  // file_info[lo].rec_off <= r
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (q.file_info[uint64_t(mid) * kFileInfoWords + kFiRecOff] <= r) lo = mid;
+      else hi = mid;
+    }
+    const uint64_t *row = q.file_info + uint64_t(lo) * kFileInfoWords;
+    const IndexFile F = q.files[lo];
+    const BatchQueryGroup g = q.groups[row[kFiQuery] < uint64_t(q.num_groups) ? row[kFiQuery] : 0];
+    const uint64_t i = r - row[kFiRecOff];
+    const uint64_t lines = row[kFiLines];
+    int32_t *o = q.out + row[kFiOutOff] + i * uint64_t(g.num_results) * 2u;
+    for (int k = 0; k < 2 * g.num_results; ++k) o[k] = -1;
+    if (F.n == 0) continue;
+    const int64_t *nl = q.NL + row[kFiNlOff];
+    const int64_t start = nl[i];
+    const int64_t end = (i + 1 < lines) ? nl[i + 1] : int64_t(F.n) - 1;
+    const Rec c{q.in + F.in_off, int64_t(F.n), q.S + F.s_off, q.LB + F.lb_off,
+                int64_t((F.n + 63u) / 64u), s_ir + g.ir_off, g.ir_len, g.base_level, F.levels};
+    run_record<int32_t>(c, start, end, g.num_results, o);
+  }
+}
+
 }  // namespace
+
+cudaError_t batch_query_launch(const BatchQueryLaunch &q, const IrBlob &ir, int grid,
+                               int block, cudaStream_t stream) {
+  batch_query_kernel<<<grid, block, 0, stream>>>(q, ir);
+  return cudaGetLastError();
+}
 
 cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
                          int block, cudaStream_t stream) {

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "indexer.cuh"
+
 namespace gpjb {
 
 constexpr int kMaxQueryLevels = 16;   // orig.hpp:10 kMaxQueryLevels
@@ -35,5 +37,34 @@ struct IrBlob {
 
 cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
                          int block, cudaStream_t stream);
+
+// Batched query over every record of every file of a multi-file index build:
+// record r belongs to the file whose record range holds it (file_info from
+// index_finalize_files); the file's query group selects the IR (packed in the
+// IrBlob), slot count and record level.  The record count is read on the
+// device, so the launch needs no host round trip.
+constexpr int kMaxBatchGroups = 8;
+struct BatchQueryGroup {
+  int ir_off = 0;
+  int ir_len = 0;
+  int num_results = 0;
+  int base_level = 0;
+};
+struct BatchQueryLaunch {
+  const uint8_t *in = nullptr;
+  const uint64_t *S = nullptr;
+  const uint64_t *LB = nullptr;
+  const int64_t *NL = nullptr;
+  const IndexFile *files = nullptr;
+  uint32_t num_files = 0;
+  const uint64_t *file_info = nullptr;  // kFileInfoWords per file
+  const uint64_t *totals = nullptr;
+  int32_t *out = nullptr;
+  int num_groups = 0;
+  BatchQueryGroup groups[kMaxBatchGroups];
+};
+
+cudaError_t batch_query_launch(const BatchQueryLaunch &q, const IrBlob &ir, int grid,
+                               int block, cudaStream_t stream);
 
 }  // namespace gpjb

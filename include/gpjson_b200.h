@@ -176,6 +176,90 @@ int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes,
                    int32_t *const *h_out, const uint64_t *out_capacity,
                    uint64_t *num_lines, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched path: many files indexed and queried by one launch chain         */
+/* ------------------------------------------------------------------------ */
+
+#define GPJ_BATCH_AUTOTUNE 4u /* time the launch shapes at creation, keep the fastest */
+#define GPJ_BATCH_NO_GRAPH 8u /* launch the kernels directly instead of a CUDA graph */
+
+/* One file of a batch: `offset` (a multiple of 128) and `size_bytes` inside
+ * the batch's device buffer; `query` indexes the batch's query table. */
+typedef struct gpj_batch_file {
+  uint64_t offset;
+  uint64_t size_bytes;
+  uint32_t query;
+  uint32_t reserved;
+} gpj_batch_file;
+
+/* A compiled query applied to every record of the files that name it.
+ * num_levels = bitmap levels indexed for those files; base_level as in
+ * gpj_query_opts. */
+typedef struct gpj_batch_query {
+  const uint8_t *h_ir;
+  uint64_t ir_len;
+  uint32_t num_result_slots;
+  uint32_t base_level;
+  uint32_t num_levels;
+  uint32_t reserved;
+} gpj_batch_query;
+
+/* Device-resident outputs of a batch (owned by the batch).
+ * d_file_info: 8 uint64 per file: lines, first newline-index slot, first
+ * record, first result int, final in-string state, final depth, size, query.
+ * d_newline: every file's newline index packed (file f at its slot);
+ * d_results: int32 [lines][slots][2] per file at its first result int, with
+ * file-local offsets; d_string/d_leveled: per-file words at the offsets of
+ * gpj_batch_file_layout.  d_totals: records, result ints, newline slots,
+ * error bits (nonzero: a bounded device wait gave up). */
+typedef struct gpj_batch_view {
+  uint64_t *d_string;
+  uint64_t *d_leveled;
+  int64_t *d_newline;
+  int32_t *d_results;
+  uint64_t *d_file_info;
+  uint64_t *d_totals;
+  uint64_t num_files;
+  uint64_t num_records;
+  uint64_t result_ints;
+  uint64_t newline_slots;
+  uint64_t string_words;
+  uint64_t leveled_words;
+  uint32_t num_tiles;
+  uint32_t index_threads; /* indexer CTA size: tiles of index_threads * 128 B */
+  uint32_t query_block;
+  uint32_t query_grid;
+  uint32_t uses_graph;
+  uint32_t reserved;
+} gpj_batch_view;
+
+typedef struct gpj_batch gpj_batch;
+
+/* Plans a batch over a 16-byte aligned device buffer: sizes every output
+ * with one run (the only host round trip), optionally autotunes the launch
+ * shapes, and captures index -> per-file finalize -> query in a CUDA graph.
+ * Replaces the per-partition loop of gpjson::Engine::query
+ * (src/gpjson/engine.cpp:131-166) run once per file, for many files at once;
+ * the batching itself has no counterpart in the reference. */
+int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
+                     const gpj_batch_file *files, uint32_t num_files,
+                     const gpj_batch_query *queries, uint32_t num_queries,
+                     uint32_t flags, gpj_batch **out, void *stream);
+
+/* Replays the batch on `stream` (asynchronous). */
+int gpj_batch_run(gpj_batch *batch, void *stream);
+
+/* Device pointers and sizes of the batch outputs. */
+int gpj_batch_view_get(const gpj_batch *batch, gpj_batch_view *view);
+
+/* Word offsets of one file's string-mask and leveled-bitmap words
+ * (leveled words are level-major with the file's own word count). */
+int gpj_batch_file_layout(const gpj_batch *batch, uint32_t file,
+                          uint64_t *string_off, uint64_t *leveled_off,
+                          uint32_t *num_levels);
+
+int gpj_batch_destroy(gpj_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,109 @@
+"""Batched path (many files, one captured launch chain) vs the CPU oracle run
+file by file: every file's string mask, leveled bitmaps, newline index and
+query results must be bit-identical."""
+import random
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from devmem import d2h
+
+pytestmark = pytest.mark.gpu
+
+QUERIES = [("$.user.lang", 0), ("$.categoryPath[1:3].id", 1), ("$.a[0:3].b", 0)]
+
+
+def _files(seed: int, count: int):
+    from gpjson_b200 import datagen
+    rng = random.Random(seed)
+    out = []
+    for i in range(count):
+        kind = i % 3
+        size = rng.choice([0, 1, 50, 127, 128, 129, 1000, 5000, 40000, 70000, 250000])
+        if kind == 0:
+            data = bytes(datagen.tweets(seed * 1000 + i, max(size, 1)))[:max(size * 3, 2000)]
+        elif kind == 1:
+            data = bytes(datagen.products(seed * 1000 + i, max(size, 3)))
+        else:
+            data = bytes(rng.choices(b'{}[]:,"\\\n ab', weights=[6, 6, 3, 3, 5, 5, 8, 1, 2, 3, 8, 8],
+                                     k=size))
+        if size == 0:
+            data = b""
+        out.append((data, kind))
+    return out
+
+
+def _run_batch(gpj, files, flags, runs=1):
+    comp = [(gpj.compile(q), base) for q, base in QUERIES]
+    queries = [(c, base, c.max_depth + base) for c, base in comp]
+    buf, offsets = gpj.pack_files([d for d, _ in files])
+    dev = torch.from_numpy(buf).cuda()
+    table = [(o, len(d), k) for o, (d, k) in zip(offsets, files)]
+    with gpj.Batch(dev.data_ptr(), buf.size, table, queries, flags=flags) as b:
+        for _ in range(runs):
+            b.run()
+        torch.cuda.synchronize()
+        v = b.view()
+        info = d2h(v.d_file_info, v.num_files * gpj.FILE_INFO_WORDS, np.uint64).reshape(-1, 8)
+        totals = d2h(v.d_totals, 4, np.uint64)
+        out = {
+            "info": info, "totals": totals, "view": (v.num_records, v.result_ints, v.uses_graph,
+                                                     v.index_threads, v.query_block),
+            "S": d2h(v.d_string, v.string_words, np.uint64),
+            "LB": d2h(v.d_leveled, v.leveled_words, np.uint64),
+            "NL": d2h(v.d_newline, v.newline_slots, np.int64),
+            "R": d2h(v.d_results, v.result_ints, np.int32),
+            "layout": [b.file_layout(f) for f in range(len(files))],
+        }
+    return comp, queries, out
+
+
+def _check(files, comp, queries, got):
+    assert got["totals"][3] == 0
+    for f, (data, kind) in enumerate(files):
+        c, base, levels = queries[kind]
+        row = got["info"][f]
+        want = oracle.OracleIndex(data, levels)
+        lines, nl_off, rec_off, out_off = (int(x) for x in row[:4])
+        assert lines == want.num_lines, f
+        np.testing.assert_array_equal(got["NL"][nl_off:nl_off + lines], want.NL, err_msg=str(f))
+        s_off, lb_off, lv = got["layout"][f]
+        W = (len(data) + 63) // 64
+        np.testing.assert_array_equal(got["S"][s_off:s_off + W], want.S, err_msg=str(f))
+        np.testing.assert_array_equal(got["LB"][lb_off:lb_off + W * lv], want.LB, err_msg=str(f))
+        slots = c.num_result_slots
+        res = got["R"][out_off:out_off + lines * slots * 2].astype(np.int64).reshape(lines, slots, 2)
+        if len(data):
+            np.testing.assert_array_equal(res, want.query(c.ir_bytes, slots, base), err_msg=str(f))
+        else:
+            assert (res == -1).all()
+
+
+def test_batch_matches_oracle_per_file(gpj):
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    files = _files(1, 60)
+    comp, queries, got = _run_batch(gpj, files, flags=0, runs=2)
+    assert got["view"][2] == 1  # graph captured
+    _check(files, comp, queries, got)
+
+
+def test_batch_without_graph_and_autotuned(gpj):
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    files = _files(2, 40)
+    comp, queries, a = _run_batch(gpj, files, flags=gpj.GPJ_BATCH_NO_GRAPH)
+    _, _, b = _run_batch(gpj, files, flags=gpj.GPJ_BATCH_AUTOTUNE)
+    _check(files, comp, queries, a)
+    _check(files, comp, queries, b)
+    assert b["view"][3] in (128, 256) and b["view"][4] in (128, 256)
+
+
+def test_batch_single_large_file_equals_plain_build(gpj, cuda_ctx):
+    from gpjson_b200 import datagen
+    data = datagen.products(5, 3 << 20)
+    files = [(bytes(data), 1)]
+    comp, queries, got = _run_batch(gpj, files, flags=0)
+    _check(files, comp, queries, got)
