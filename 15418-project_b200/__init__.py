@@ -46,9 +46,11 @@ EXPORTED_SYMBOLS = (
     "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_build_noalloc",
     "gpj_index_free",
     "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
-    "gpj_batch_create", "gpj_batch_run", "gpj_batch_view_get", "gpj_batch_file_layout",
-    "gpj_batch_destroy",
+    "gpj_batch_create", "gpj_batch_run", "gpj_batch_run_stages", "gpj_batch_run_per_file",
+    "gpj_batch_run_host",
+    "gpj_batch_view_get", "gpj_batch_file_layout", "gpj_batch_destroy",
 )
+STAGE_INDEX, STAGE_FINALIZE, STAGE_QUERY = 1, 2, 4
 
 GPJ_BATCH_AUTOTUNE = 4
 GPJ_BATCH_NO_GRAPH = 8
@@ -193,6 +195,9 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_batch_create.argtypes = [vp, vp, u64, P(BatchFile), u32, P(BatchQuery), u32, u32,
                                      P(vp), vp]
     lib.gpj_batch_run.argtypes = [vp, vp]
+    lib.gpj_batch_run_stages.argtypes = [vp, u32, vp]
+    lib.gpj_batch_run_per_file.argtypes = [vp, vp]
+    lib.gpj_batch_run_host.argtypes = [vp, vp, vp, vp, vp]
     lib.gpj_batch_view_get.argtypes = [vp, P(BatchView)]
     lib.gpj_batch_file_layout.argtypes = [vp, u32, P(u64), P(u64), P(u32)]
     lib.gpj_batch_destroy.argtypes = [vp]
@@ -369,6 +374,17 @@ class Batch:
 
     def run(self, stream: int = 0) -> None:
         _check(self._lib.gpj_batch_run(self._h, C.c_void_p(stream)))
+
+    def run_stages(self, stages: int, stream: int = 0) -> None:
+        _check(self._lib.gpj_batch_run_stages(self._h, stages, C.c_void_p(stream)))
+
+    def run_per_file(self, stream: int = 0) -> None:
+        _check(self._lib.gpj_batch_run_per_file(self._h, C.c_void_p(stream)))
+
+    def run_host(self, h_input: int, h_results: int = 0, h_file_info: int = 0,
+                 stream: int = 0) -> None:
+        _check(self._lib.gpj_batch_run_host(self._h, C.c_void_p(h_input), C.c_void_p(h_results),
+                                            C.c_void_p(h_file_info), C.c_void_p(stream)))
 
     def view(self) -> BatchView:
         v = BatchView()

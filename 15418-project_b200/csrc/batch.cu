@@ -36,6 +36,9 @@ struct gpj_batch {
   int max_levels = 0;
   // device state
   gpjb::IndexFile *d_files = nullptr;
+  uint32_t *d_tile_file = nullptr;
+  std::vector<uint64_t> host_lines;  // per-file line counts (sizing pass)
+  std::vector<uint64_t> host_info;   // file info rows of the sizing pass
   uint32_t *d_query_of_file = nullptr;
   uint32_t *d_slots = nullptr;
   uint64_t *d_S = nullptr, *d_LB = nullptr;
@@ -94,6 +97,7 @@ int bind_launch(gpj_batch *b) {
   L.in = b->d_input;
   L.full_rows = b->input_bytes / 128u;
   L.files = b->d_files;
+  L.tile_file = b->d_tile_file;
   L.num_files = b->num_files;
   L.num_levels = b->max_levels;
   L.S = b->d_S;
@@ -141,6 +145,7 @@ void release(gpj_batch *b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->stream) cudaStreamDestroy(b->stream);
   cudaFree(b->d_files);
+  cudaFree(b->d_tile_file);
   cudaFree(b->d_query_of_file);
   cudaFree(b->d_slots);
   cudaFree(b->d_S);
@@ -157,9 +162,11 @@ int alloc_layout_buffers(gpj_batch *b) {
   cudaFree(b->d_LB);
   cudaFree(b->d_scratch);
   cudaFree(b->d_files);
+  cudaFree(b->d_tile_file);
   b->d_S = b->d_LB = nullptr;
   b->d_scratch = nullptr;
   b->d_files = nullptr;
+  b->d_tile_file = nullptr;
   BCUDA(cudaMalloc(&b->d_S, (b->s_words + 2) * 8u), "cudaMalloc S");
   BCUDA(cudaMalloc(&b->d_LB, (b->lb_words + 2) * 8u), "cudaMalloc LB");
   BCUDA(cudaMalloc(&b->d_scratch, (uint64_t(b->L.num_tiles) * 8u + 64u + 255u) & ~uint64_t(255)),
@@ -168,6 +175,15 @@ int alloc_layout_buffers(gpj_batch *b) {
   BCUDA(cudaMemcpy(b->d_files, b->files.data(), b->files.size() * sizeof(gpjb::IndexFile),
                    cudaMemcpyHostToDevice),
         "copy file table");
+  std::vector<uint32_t> tile_file(b->L.num_tiles);
+  for (uint32_t f = 0; f < b->num_files; ++f) {
+    const uint32_t end = (f + 1 < b->num_files) ? b->files[f + 1].first_tile : b->L.num_tiles;
+    for (uint32_t t = b->files[f].first_tile; t < end; ++t) tile_file[t] = f;
+  }
+  BCUDA(cudaMalloc(&b->d_tile_file, (tile_file.size() + 1) * 4u), "cudaMalloc tile map");
+  BCUDA(cudaMemcpy(b->d_tile_file, tile_file.data(), tile_file.size() * 4u,
+                   cudaMemcpyHostToDevice),
+        "copy tile map");
   return bind_launch(b);
 }
 
@@ -282,6 +298,11 @@ int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
     b->records = totals[gpjb::kTotRecords];
     b->result_ints = totals[gpjb::kTotResultInts];
     b->nl_slots = totals[gpjb::kTotNlSlots];
+    std::vector<uint64_t> info(uint64_t(num_files) * gpjb::kFileInfoWords);
+    if (cudaMemcpy(info.data(), b->d_info, info.size() * 8u, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return bail(fail_cuda(cudaErrorUnknown, "read file info"));
+    b->host_lines.resize(num_files);
+    b->host_info = info;
   }
   if (cudaMalloc(&b->d_NL, (b->nl_slots + 1) * 8u) != cudaSuccess ||
       cudaMalloc(&b->d_out, (b->result_ints + 1) * 4u) != cudaSuccess)
@@ -349,6 +370,100 @@ int gpj_batch_run(gpj_batch *b, void *stream_) {
   } else {
     BCUDA(enqueue(b, stream, true), "batch launch");
   }
+  return GPJ_OK;
+}
+
+int gpj_batch_run_stages(gpj_batch *b, uint32_t stages, void *stream_) {
+  if (b == nullptr) return gpjb::report_error(GPJ_ERR_INVALID_ARGUMENT, "null batch");
+  auto stream = static_cast<cudaStream_t>(stream_);
+  BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
+  if (stages & GPJ_BATCH_STAGE_INDEX)
+    BCUDA(gpjb::index_launch(b->L, b->tma ? &b->map : nullptr, b->tma, stream, b->index_threads),
+          "batch index launch");
+  if (stages & GPJ_BATCH_STAGE_FINALIZE)
+    BCUDA(gpjb::index_finalize_files(b->L, b->d_query_of_file, b->d_slots, b->d_info,
+                                     b->d_totals, stream),
+          "batch finalize launch");
+  if (stages & GPJ_BATCH_STAGE_QUERY)
+    BCUDA(gpjb::batch_query_launch(query_launch_of(b), b->blob, b->query_grid, b->query_block,
+                                   stream),
+          "batch query launch");
+  return GPJ_OK;
+}
+
+int gpj_batch_run_per_file(gpj_batch *b, void *stream_) {
+  if (b == nullptr) return gpjb::report_error(GPJ_ERR_INVALID_ARGUMENT, "null batch");
+  auto stream = static_cast<cudaStream_t>(stream_);
+  BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
+  // one single-file launch chain per file (the per-partition loop of a
+  // plain caller), writing the same outputs at the same places
+  for (uint32_t f = 0; f < b->num_files; ++f) {
+    const gpjb::IndexFile &F = b->files[f];
+    const uint64_t *row = b->host_info.data() + uint64_t(f) * gpjb::kFileInfoWords;
+    const gpjb::BatchQueryGroup &G = b->groups[b->query_of_file[f]];
+    gpjb::IndexLaunch L;
+    L.in = b->d_input + F.in_off;
+    L.single.n = F.n;
+    L.single.levels = F.levels;
+    L.num_levels = F.levels;
+    L.full_rows = F.n / 128u;
+    L.S = b->d_S + F.s_off;
+    L.LB = b->d_LB + F.lb_off;
+    L.NL = b->d_NL + row[gpjb::kFiNlOff];
+    L.nl_cap = row[gpjb::kFiLines];
+    L.num_tiles = uint32_t(gpjb::index_num_tiles(F.n));
+    gpjb::index_bind_scratch(L, b->d_scratch);
+    if (F.n == 0) {  // one empty record: NL = [0], every slot -1
+      BCUDA(cudaMemsetAsync(L.NL, 0, 8, stream), "cudaMemsetAsync");
+      BCUDA(cudaMemsetAsync(b->d_out + row[gpjb::kFiOutOff], 0xFF,
+                            size_t(G.num_results) * 8u, stream),
+            "cudaMemsetAsync");
+      continue;
+    }
+    CUtensorMap map;
+    const bool tma = (b->flags & GPJ_INDEX_NO_TMA) == 0 &&
+                     gpjb::index_make_tensor_map(&map, L.in, F.n);
+    BCUDA(gpjb::index_launch(L, tma ? &map : nullptr, tma, stream), "per-file index launch");
+    gpjb::QueryLaunch q;
+    q.in = L.in;
+    q.n = int64_t(F.n);
+    q.NL = L.NL;
+    q.num_lines = int64_t(row[gpjb::kFiLines]);
+    q.S = L.S;
+    q.LB = L.LB;
+    q.W = int64_t((F.n + 63u) / 64u);
+    q.ir_len = G.ir_len;
+    q.num_results = G.num_results;
+    q.num_levels = F.levels;
+    q.base_level = G.base_level;
+    q.out32 = b->d_out + row[gpjb::kFiOutOff];
+    gpjb::IrBlob blob;
+    std::memcpy(blob.bytes, b->blob.bytes + G.ir_off, size_t(G.ir_len));
+    BCUDA(gpjb::query_launch(q, blob, 0, 256, stream), "per-file query launch");
+  }
+  return GPJ_OK;
+}
+
+int gpj_batch_run_host(gpj_batch *b, const uint8_t *h_input, int32_t *h_results,
+                       uint64_t *h_file_info, void *stream_) {
+  if (b == nullptr || h_input == nullptr)
+    return gpjb::report_error(GPJ_ERR_INVALID_ARGUMENT, "null batch or input");
+  auto stream = static_cast<cudaStream_t>(stream_);
+  BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
+  BCUDA(cudaMemcpyAsync(const_cast<uint8_t *>(b->d_input), h_input, b->input_bytes,
+                        cudaMemcpyHostToDevice, stream),
+        "copy batch input");
+  const int rc = gpj_batch_run(b, stream_);
+  if (rc != GPJ_OK) return rc;
+  if (h_results != nullptr && b->result_ints > 0)
+    BCUDA(cudaMemcpyAsync(h_results, b->d_out, b->result_ints * 4u, cudaMemcpyDeviceToHost,
+                          stream),
+          "copy batch results");
+  if (h_file_info != nullptr)
+    BCUDA(cudaMemcpyAsync(h_file_info, b->d_info, uint64_t(b->num_files) * 64u,
+                          cudaMemcpyDeviceToHost, stream),
+          "copy batch file info");
+  BCUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
   return GPJ_OK;
 }
 

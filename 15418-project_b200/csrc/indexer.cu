@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(NT)
       s_file_idx = 0;
       s_file = P.single;
     } else if (t < P.num_tiles) {
-      const uint32_t f = file_of_tile(P, t);
+      const uint32_t f = P.tile_file ? P.tile_file[t] : file_of_tile(P, t);
       s_file_idx = f;
       s_file = P.files[f];
     }

@@ -34,6 +34,7 @@ struct IndexLaunch {
   uint64_t full_rows = 0;       // whole 128-byte rows of `in` the TMA descriptor covers
   IndexFile single;             // the file when `files` is null (one partition)
   const IndexFile *files = nullptr;  // device table, num_files entries, or null
+  const uint32_t *tile_file = nullptr;  // file of each tile (optional; else binary search)
   uint32_t num_files = 1;
   int num_levels = 0;           // max L over the files (selects the kernel)
   uint64_t *S = nullptr;        // string mask words

@@ -24,6 +24,14 @@ enum : uint8_t {
   OP_EXPRESSION_STRING_EQUALS = 0x09,
 };
 
+// Last bitmap word read, per thread: consecutive searches of a record mostly
+// start in the word the previous search ended in.
+struct WordCache {
+  const uint64_t *bm = nullptr;
+  int64_t idx = -1;
+  uint64_t val = 0;
+};
+
 struct Rec {
   const uint8_t *in;
   int64_t n;
@@ -49,17 +57,27 @@ __device__ __forceinline__ uint8_t ir_at(const Rec &c, int64_t i) {
   return (i >= 0 && i < c.ir_len) ? c.ir[i] : uint8_t(0);
 }
 
+__device__ __forceinline__ uint64_t cached_word(WordCache &wc, const uint64_t *bm, int64_t W,
+                                                int64_t i) {
+  if (wc.bm == bm && wc.idx == i) return wc.val;
+  const uint64_t v = word_at(bm, W, i);
+  wc.bm = bm;
+  wc.idx = i;
+  wc.val = v;
+  return v;
+}
+
 __device__ __forceinline__ uint64_t mask_through_bit(int b) {
   return b == 63 ? ~0ull : ((1ull << (b + 1)) - 1ull);
 }
 
 // query.cu:39-77
-__device__ int64_t prev_bit(const uint64_t *bm, int64_t W, int64_t min_index,
+__device__ int64_t prev_bit(WordCache &wc, const uint64_t *bm, int64_t W, int64_t min_index,
                             int64_t line_index) {
   if (line_index < min_index) return -1;
   int64_t wi = line_index >> 6;
   int64_t base = wi * 64;
-  uint64_t word = word_at(bm, W, wi) & mask_through_bit(int(line_index - base));
+  uint64_t word = cached_word(wc, bm, W, wi) & mask_through_bit(int(line_index - base));
   while (base + 63 >= min_index) {
     uint64_t cand = word;
     const int64_t first = min_index - base;
@@ -69,13 +87,13 @@ __device__ int64_t prev_bit(const uint64_t *bm, int64_t W, int64_t min_index,
     --wi;
     base -= 64;
     if (base + 63 < min_index) break;
-    word = word_at(bm, W, wi);
+    word = cached_word(wc, bm, W, wi);
   }
   return -1;
 }
 
 // query.cu:79-115
-__device__ int64_t next_struct(const Rec &c, int64_t level_end,
+__device__ int64_t next_struct(const Rec &c, WordCache &wc, int64_t level_end,
                                int64_t line_index, int level) {
   if (line_index >= level_end) return level_end;
   // a level the index does not hold has no structural characters
@@ -83,7 +101,7 @@ __device__ int64_t next_struct(const Rec &c, int64_t level_end,
   const uint64_t *lvl = c.LB + uint64_t(c.W) * uint64_t(level + c.base);
   int64_t wi = line_index >> 6;
   int64_t base = wi * 64;
-  uint64_t word = word_at(lvl, c.W, wi) & (~0ull << (line_index - base));
+  uint64_t word = cached_word(wc, lvl, c.W, wi) & (~0ull << (line_index - base));
   while (base <= level_end) {
     uint64_t cand = word;
     const int64_t last = level_end - base;
@@ -92,18 +110,18 @@ __device__ int64_t next_struct(const Rec &c, int64_t level_end,
     ++wi;
     base += 64;
     if (base > level_end) break;
-    word = word_at(lvl, c.W, wi);
+    word = cached_word(wc, lvl, c.W, wi);
   }
   return level_end;
 }
 
 // query.cu:117-128
-__device__ int64_t prev_struct(const Rec &c, int64_t level_start,
+__device__ int64_t prev_struct(const Rec &c, WordCache &wc, int64_t level_start,
                                int64_t line_index, int level) {
   if (line_index <= level_start) return level_start;
   if (level + c.base < 0 || level + c.base >= c.levels) return level_start;
   const uint64_t *lvl = c.LB + uint64_t(c.W) * uint64_t(level + c.base);
-  const int64_t s = prev_bit(lvl, c.W, level_start, line_index);
+  const int64_t s = prev_bit(wc, lvl, c.W, level_start, line_index);
   return s == -1 ? level_start : s;
 }
 
@@ -139,6 +157,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
   // forever, and the record is abandoned instead.
   const int64_t max_steps = (line_end - line_start) + 2;
   int64_t steps = 0;
+  WordCache lbc, sc;  // leveled-bitmap and string-mask words
   int64_t level_end[kMaxQueryLevels];
   level_end[0] = line_end;
 #pragma unroll
@@ -182,7 +201,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       ++level;
       if (!LEVEL_OK(level) || level < 1) return;
       if (level_end[level] == -1) {
-        level_end[level] = next_struct(c, level_end[level - 1], line_index + 1, level - 1);
+        level_end[level] = next_struct(c, lbc, level_end[level - 1], line_index + 1, level - 1);
         while (at(c, line_index) == ' ') ++line_index;
       }
       break;
@@ -196,9 +215,9 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       for (;;) {
         if (++steps > max_steps) return;
         ++line_index;
-        line_index = next_struct(c, level_end[level], line_index, level);
+        line_index = next_struct(c, lbc, level_end[level], line_index, level);
         if (at(c, line_index) == ':') {
-          const int64_t string_end = prev_bit(c.S, c.W, line_start + 1, line_index - 1);
+          const int64_t string_end = prev_bit(sc, c.S, c.W, line_start + 1, line_index - 1);
           const int64_t string_start = string_end - key_len;
           bool mismatch = string_start < line_start || at(c, string_start) != '"';
           for (int i = 0; !mismatch && i < key_len; ++i) {
@@ -206,7 +225,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
           }
           if (mismatch) {
             ++line_index;
-            line_index = next_struct(c, level_end[level], line_index, level);
+            line_index = next_struct(c, lbc, level_end[level], line_index, level);
             if (at(c, line_index) == '}') return;
             continue;
           }
@@ -227,7 +246,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
         if (++steps > max_steps) return;
         if (curr_index[level] < target) {
           ++line_index;
-          line_index = next_struct(c, level_end[level], line_index, level);
+          line_index = next_struct(c, lbc, level_end[level], line_index, level);
           if (at(c, line_index) == ',') {
             ++curr_index[level];
             continue;
@@ -236,7 +255,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
         }
         if (curr_index[level] > target) {
           --line_index;
-          line_index = prev_struct(c, 0, line_index, level);
+          line_index = prev_struct(c, lbc, 0, line_index, level);
           --curr_index[level];
           continue;
         }
@@ -260,7 +279,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
         if (++steps > max_steps) return;
         if (curr_index[level] < target) {
           --line_index;
-          line_index = prev_struct(c, 0, line_index, level);
+          line_index = prev_struct(c, lbc, 0, line_index, level);
           if (at(c, line_index) == ',' || curr_index[level] + 1 == target) {
             ++curr_index[level];
             continue;
@@ -269,7 +288,7 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
         }
         if (curr_index[level] > target) {
           ++line_index;
-          line_index = next_struct(c, level_end[level], line_index, level);
+          line_index = next_struct(c, lbc, level_end[level], line_index, level);
           --curr_index[level];
           continue;
         }

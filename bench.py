@@ -41,6 +41,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+sys.path.insert(0, str(ROOT / "tests"))
 import __graft_entry__ as entry  # noqa: E402
 
 METRIC = "index+query GB/s"
@@ -66,6 +67,8 @@ def workload(name: str, pkg, size_mib: int | None = None):
         queries, records = ["$[*].categoryPath[1:3].id"], "array"
         desc = ("c1: 1 GiB single top-level array of ~2 KiB product records, "
                 "$[*].categoryPath[1:3].id")
+    elif name == "c3":
+        raise SystemExit("c3 is a batch workload: see run_batch")
     elif name == "c2":
         data = dg.tweets(2, 4 << 30, deep=True)
         queries = ["$.user.lang", "$.entities.hashtags[*].text", "$.place.country_code",
@@ -75,6 +78,52 @@ def workload(name: str, pkg, size_mib: int | None = None):
     else:
         raise SystemExit(f"unknown workload {name}")
     return data, queries, records, desc
+
+
+def c3_sizes(seed: int = 3, count: int = 10_000, total: int = 8 << 30,
+             lo: int = 4 << 10, hi: int = 64 << 20, sigma: float = 2.0):
+    """File sizes: ln(size) ~ N(mu, sigma) truncated to [lo, hi], mu solved so
+    that the truncated mean is total / count."""
+    from math import erf, exp, log, sqrt
+
+    def phi(x):
+        return 0.5 * (1.0 + erf(x / sqrt(2.0)))
+
+    def tmean(mu):
+        a, b = (log(lo) - mu) / sigma, (log(hi) - mu) / sigma
+        return exp(mu + sigma * sigma / 2) * (phi(b - sigma) - phi(a - sigma)) / (phi(b) - phi(a))
+
+    target = total / count
+    m0, m1 = log(lo), log(hi)
+    for _ in range(100):
+        mid = 0.5 * (m0 + m1)
+        if tmean(mid) < target:
+            m0 = mid
+        else:
+            m1 = mid
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        x = rng.lognormal(0.5 * (m0 + m1), sigma, size=count)
+        out.extend(int(v) for v in x if lo <= v <= hi)
+    sizes = np.array(out[:count], np.int64)
+    sizes[-1] = int(np.clip(sizes[-1] + (total - sizes.sum()), lo, hi))
+    return sizes
+
+
+def c3_files(pkg, scale: float = 1.0):
+    """10,000 seeded files (even: NDJSON post records, odd: product arrays)."""
+    sizes = c3_sizes(total=int((8 << 30) * scale)) if scale != 1.0 else c3_sizes()
+    dg = pkg.datagen
+
+    def make(i):
+        n = int(sizes[i])
+        if i % 2 == 0:
+            return bytes(dg.tweets(3_000_000 + i, n)), 0
+        return bytes(dg.products(4_000_000 + i, n)), 1
+
+    with cf.ThreadPoolExecutor(os.cpu_count() or 4) as pool:
+        return list(pool.map(make, range(len(sizes))))
 
 
 def compile_all(pkg, queries):
@@ -319,6 +368,158 @@ def run_ours(args, world, rank, local):
     return line
 
 
+def run_batch(args, world, rank, local):
+    """c3: 10,000 files (8 GiB) indexed and queried by one captured launch
+    chain (gpj_batch), next to the plain one-launch-chain-per-file path."""
+    import torch
+    pkg = entry.package()
+    pkg.load_library()
+    files = c3_files(pkg, args.scale)
+    qtext = ["$.user.lang", "$[*].categoryPath[1:3].id"]
+    comp = compile_all(pkg, qtext)
+    queries = [(c, base, c.max_depth + base) for c, base in comp]
+    buf, offsets = pkg.pack_files([d for d, _ in files])
+    total = sum(len(d) for d, _ in files)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    s = stream.cuda_stream
+    d_buf = torch.from_numpy(buf).to(dev)
+    table = [(o, len(d), k) for o, (d, k) in zip(offsets, files)]
+    batch = pkg.Batch(d_buf.data_ptr(), buf.size, table, queries, flags=pkg.GPJ_BATCH_AUTOTUNE)
+    v = batch.view()
+
+    def timed(fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for e0, e1 in ev:
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return float(np.mean([e0.elapsed_time(e1) for e0, e1 in ev]))
+
+    for _ in range(args.warmup):
+        batch.run(s)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local)
+    barrier(world)
+    clocks.start()
+    ms_step = timed(lambda: batch.run(s), args.steps)
+    clk = clocks.stop()
+    barrier(world)
+    ms_step = allreduce_max(ms_step, world)
+    ms_index = allreduce_max(timed(lambda: batch.run_stages(pkg.STAGE_INDEX, s), 3), world)
+    ms_query = allreduce_max(timed(lambda: batch.run_stages(pkg.STAGE_QUERY, s), 3), world)
+    from devmem import d2h
+    info = d2h(v.d_file_info, v.num_files * pkg.FILE_INFO_WORDS, np.uint64).reshape(-1, 8)
+    assert int(d2h(v.d_totals, 4, np.uint64)[3]) == 0
+    lines = info[:, 0].astype(np.int64)
+    levels = np.array([queries[k][2] for _, k in files], np.int64)
+    nbytes = np.array([len(d) for d, _ in files], np.int64)
+    W = (nbytes + 63) // 64
+    b_index = int((nbytes + 8 * W * (1 + levels) + 8 * lines).sum())
+    b_query = int(v.result_ints) * 4
+
+    # plain path: one single-file index launch + one query launch per file,
+    # issued from C (gpj_batch_run_per_file), into the same outputs
+    want = torch.from_numpy(d2h(v.d_results, v.result_ints, np.int32))
+    batch.run_per_file(s)
+    torch.cuda.synchronize(dev)
+    ms_plain = allreduce_max(timed(lambda: batch.run_per_file(s), 3), world)
+    got = torch.from_numpy(d2h(v.d_results, v.result_ints, np.int32))
+    assert torch.equal(got, want), "plain per-file results differ from the batch"
+
+    # end to end: host input in, host results out, through gpj_batch_run_host
+    h_in = torch.from_numpy(buf).pin_memory()
+    h_out = torch.empty(int(v.result_ints) + 1, dtype=torch.int32).pin_memory()
+    h_info = torch.empty(v.num_files * pkg.FILE_INFO_WORDS, dtype=torch.int64).pin_memory()
+    for _ in range(1):
+        batch.run_host(h_in.data_ptr(), h_out.data_ptr(), h_info.data_ptr(), s)
+    e2e = []
+    for _ in range(max(2, min(args.steps, 5))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.run_host(h_in.data_ptr(), h_out.data_ptr(), h_info.data_ptr(), s)
+        e1.record(stream)
+        e1.synchronize()
+        e2e.append(e0.elapsed_time(e1))
+    assert torch.equal(h_out[: int(v.result_ints)], want)
+    e2e_ms = allreduce_max(float(np.mean(e2e)), world)
+
+    gb = total * world / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    achieved = b_index / (ms_index / 1e3) / 1e9
+    chain = (b_index + b_query) / (ms_step / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "traffic_c3.json"
+    if tp.exists():
+        try:
+            traffic = json.loads(tp.read_text()).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": round(gb / (ms_step / 1e3), 3), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": {"workload": "c3: 10,000 seeded files, log-normal sizes 4 KiB-64 MiB, "
+                               "half NDJSON post records ($.user.lang), half product arrays "
+                               "($[*].categoryPath[1:3].id), one captured launch chain",
+                   "input_bytes": total, "files": len(files), "records": int(v.num_records),
+                   "l2": "input larger than L2", "parallelism": f"replicas x{world}",
+                   "launch_shape": {"index_threads": v.index_threads,
+                                    "query_block": v.query_block, "query_grid": v.query_grid,
+                                    "graph": bool(v.uses_graph)}},
+        "plain_per_file": {"value": round(gb / (ms_plain / 1e3), 3), "unit": "GB/s",
+                           "ms_per_step": round(ms_plain, 3),
+                           "batched_over_plain": round(ms_plain / ms_step, 2)},
+        "e2e": {"value": round(gb / (e2e_ms / 1e3), 3), "unit": "GB/s",
+                "h2d_bytes_per_step": int(buf.size),
+                "d2h_bytes_per_step": int(v.result_ints) * 4 + v.num_files * 64},
+        "gpu_launches": 3,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "kernel": "gpjb::index_kernel (batched file table)", "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": b_index, "ms_per_launch": round(ms_index, 4),
+                     "chain_achieved": round(chain, 1), "chain_frac": round(chain / peak, 4)},
+        "index_ms": round(ms_index, 4), "query_ms": round(ms_query, 4), "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_files(files, comp, queries)
+    batch.close()
+    return line
+
+
+def cpu_baseline_files(files, comp, queries, budget_bytes: int = 96 << 20):
+    """The oracle on whole files (a bounded sample), one file per task on
+    every host thread."""
+    import oracle
+    threads = os.cpu_count() or 1
+    sample, acc = [], 0
+    for d, k in files:
+        if acc >= budget_bytes:
+            break
+        sample.append((d, k))
+        acc += len(d)
+
+    def work(item):
+        d, k = item
+        c, base, lv = queries[k]
+        ix = oracle.OracleIndex(d, lv)
+        if len(d):
+            ix.query(c.ir_bytes, c.num_result_slots, base)
+        return len(d)
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as pool:
+        done = sum(pool.map(work, sample))
+    dt = time.perf_counter() - t0
+    return {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
+            "kind": "port", "sample": f"{len(sample)} whole files, {done} bytes, "
+            f"one file per task on {threads} threads"}
+
+
 def _partitions(data: np.ndarray, parts: int):
     """Newline-aligned partitions (the reference's independent partitions,
     src/gpjson/file/file_reader.cpp:41-77)."""
@@ -393,7 +594,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2"])
+    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="c3 only: fraction of the 8 GiB total (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size-mib", type=int, default=None,
                     help="profiling: run the workload's generator at this size")
@@ -402,6 +605,8 @@ def main():
     world, rank, local = dist_init()
     if args.impl == "reference":
         line = run_reference(args, world, rank)
+    elif args.workload == "c3":
+        line = run_batch(args, world, rank, local)
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0 and line is not None:

@@ -249,6 +249,25 @@ int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
 /* Replays the batch on `stream` (asynchronous). */
 int gpj_batch_run(gpj_batch *batch, void *stream);
 
+/* Runs only some stages of the batch, directly (no graph), in the order
+ * index, finalize, query: for timing and profiling one kernel. */
+#define GPJ_BATCH_STAGE_INDEX 1u
+#define GPJ_BATCH_STAGE_FINALIZE 2u
+#define GPJ_BATCH_STAGE_QUERY 4u
+int gpj_batch_run_stages(gpj_batch *batch, uint32_t stages, void *stream);
+
+/* The same work as gpj_batch_run, issued the plain way: one single-file
+ * index launch and one query launch per file, into the same outputs (the
+ * comparison point of the batched path; no host round trips). */
+int gpj_batch_run_per_file(gpj_batch *batch, void *stream);
+
+/* End to end from host memory: copies h_input (input_bytes, the batch's
+ * layout) into the batch's device input buffer, runs the batch, copies the
+ * result ints (view.result_ints) and the per-file info (8 uint64 per file)
+ * back, and waits.  Either output pointer may be NULL. */
+int gpj_batch_run_host(gpj_batch *batch, const uint8_t *h_input, int32_t *h_results,
+                       uint64_t *h_file_info, void *stream);
+
 /* Device pointers and sizes of the batch outputs. */
 int gpj_batch_view_get(const gpj_batch *batch, gpj_batch_view *view);
 

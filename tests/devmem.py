@@ -28,6 +28,8 @@ def cudart() -> C.CDLL:
                 continue
         _rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
         _rt.cudaMemcpy.restype = C.c_int
+        _rt.cudaMemset.argtypes = [C.c_void_p, C.c_int, C.c_size_t]
+        _rt.cudaMemset.restype = C.c_int
     return _rt
 
 

@@ -107,3 +107,34 @@ def test_batch_single_large_file_equals_plain_build(gpj, cuda_ctx):
     files = [(bytes(data), 1)]
     comp, queries, got = _run_batch(gpj, files, flags=0)
     _check(files, comp, queries, got)
+
+
+def test_plain_per_file_launches_match_batch(gpj):
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    files = _files(3, 30)
+    comp = [(gpj.compile(q), base) for q, base in QUERIES]
+    queries = [(c, base, c.max_depth + base) for c, base in comp]
+    buf, offsets = gpj.pack_files([d for d, _ in files])
+    dev = torch.from_numpy(buf).cuda()
+    table = [(o, len(d), k) for o, (d, k) in zip(offsets, files)]
+    with gpj.Batch(dev.data_ptr(), buf.size, table, queries) as b:
+        v = b.view()
+        b.run()
+        torch.cuda.synchronize()
+        want = [d2h(p, n, t) for p, n, t in [(v.d_results, v.result_ints, np.int32),
+                                              (v.d_newline, v.newline_slots, np.int64),
+                                              (v.d_string, v.string_words, np.uint64),
+                                              (v.d_leveled, v.leveled_words, np.uint64)]]
+        for p, n, sz in [(v.d_results, v.result_ints, 4), (v.d_newline, v.newline_slots, 8),
+                         (v.d_string, v.string_words, 8), (v.d_leveled, v.leveled_words, 8)]:
+            from devmem import cudart
+            cudart().cudaMemset(p, 0x5A, n * sz)
+        b.run_per_file()
+        torch.cuda.synchronize()
+        got = [d2h(p, n, t) for p, n, t in [(v.d_results, v.result_ints, np.int32),
+                                             (v.d_newline, v.newline_slots, np.int64),
+                                             (v.d_string, v.string_words, np.uint64),
+                                             (v.d_leveled, v.leveled_words, np.uint64)]]
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
