@@ -73,6 +73,52 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+CPP = PKG / "cpp"
+CPP_LIB = LIBDIR / "libgpjson_cpp.so"
+DRIVER = LIBDIR / "gpjson_driver"
+CXX = os.environ.get("CXX", "g++")
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-Wall", "-I", str(CPP / "include"), "-I",
+            str(ROOT / "include"), "-I", str(CUDA_HOME / "include")]
+LDCUDA = ["-L", str(CUDA_HOME / "lib64"), "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
+
+
+def build_cpp(force: bool = False, verbose: bool = False) -> Path:
+    """The reference-shaped C++ API (libgpjson_cpp.so) over the C ABI, and
+    the gpjson_driver executable."""
+    build_library(force=False, verbose=verbose)
+    srcs = sorted((CPP / "src").glob("*.cpp"))
+    deps = srcs + sorted((CPP / "src").glob("*.hpp")) + sorted((CPP / "include").rglob("*.hpp")) + \
+        [LIB]
+    if force or _stale(CPP_LIB, deps):
+        cmd = [CXX, *CXXFLAGS, "-shared", *map(str, srcs), "-o", str(CPP_LIB), "-L", str(LIBDIR),
+               "-lgpjson_b200", "-Wl,-rpath,$ORIGIN", *LDCUDA]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    app = CPP / "apps" / "gpjson_driver.cpp"
+    if force or _stale(DRIVER, [app, CPP_LIB]):
+        cmd = [CXX, *CXXFLAGS, str(app), "-o", str(DRIVER), "-L", str(LIBDIR), "-lgpjson_cpp",
+               "-lgpjson_b200", "-Wl,-rpath,$ORIGIN", *LDCUDA]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CPP_LIB
+
+
+def build_cpp_test(src_dir: Path, out: Path) -> Path:
+    """Compiles the C++ API test program (tests/cpp) against libgpjson_cpp."""
+    build_cpp()
+    srcs = sorted(src_dir.glob("*.cpp"))
+    if _stale(out, srcs + [CPP_LIB]):
+        out.parent.mkdir(parents=True, exist_ok=True)
+        subprocess.run([CXX, *CXXFLAGS, *map(str, srcs), "-o", str(out), "-L", str(LIBDIR),
+                        "-lgpjson_cpp", "-lgpjson_b200", f"-Wl,-rpath,{LIBDIR}", *LDCUDA],
+                       check=True)
+    return out
+
+
 if __name__ == "__main__":
     build_library(force="--force" in sys.argv, verbose=True)
+    build_cpp(force="--force" in sys.argv, verbose=True)
     print(LIB)

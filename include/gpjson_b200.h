@@ -20,7 +20,7 @@ extern "C" {
 #endif
 
 /* Status codes.  The C++ wrapper maps them back onto the reference's
- * exception types (include/gpjson/error/*.hpp, query/error.hpp, file/error.hpp,
+ * exception types (include/gpjson/error/ headers, query/error.hpp, file/error.hpp,
  * cuda/error.hpp). */
 #define GPJ_OK 0
 #define GPJ_ERR_CUDA 1              /* error::cuda::CudaError */
