@@ -49,6 +49,9 @@ EXPORTED_SYMBOLS = (
     "gpj_batch_create", "gpj_batch_run", "gpj_batch_run_stages", "gpj_batch_run_per_file",
     "gpj_batch_run_host",
     "gpj_batch_view_get", "gpj_batch_file_layout", "gpj_batch_destroy",
+    "gpj_server_create", "gpj_server_submit", "gpj_server_poll", "gpj_server_wait",
+    "gpj_server_response", "gpj_server_release", "gpj_server_stats_get",
+    "gpj_server_clear_cache", "gpj_server_destroy",
 )
 STAGE_INDEX, STAGE_FINALIZE, STAGE_QUERY = 1, 2, 4
 
@@ -154,6 +157,40 @@ class BatchView(C.Structure):
                 ("uses_graph", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+GPJ_SERVER_NO_CACHE = 1
+GPJ_SERVER_SLEEP_POLL = 2
+SERVER_MAX_QUERIES = 8
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("num_slots", C.c_int32),
+                ("hbm_budget_bytes", C.c_uint64), ("host_result_bytes", C.c_uint64),
+                ("cache_levels", C.c_int32), ("flags", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
+
+
+class Request(C.Structure):
+    _fields_ = [("file_key", C.c_uint64), ("h_input", C.c_void_p), ("size_bytes", C.c_uint64),
+                ("queries", C.c_void_p), ("num_queries", C.c_uint32), ("reserved", C.c_uint32),
+                ("arrival_ns", C.c_uint64)]
+
+
+class Response(C.Structure):
+    _fields_ = [("status", C.c_int32), ("cache_hit", C.c_int32), ("num_lines", C.c_uint64),
+                ("h_results", C.c_void_p), ("result_ints", C.c_uint64),
+                ("result_offset", C.c_uint64 * SERVER_MAX_QUERIES),
+                ("arrival_ns", C.c_uint64), ("admit_ns", C.c_uint64),
+                ("index_ready_ns", C.c_uint64), ("done_ns", C.c_uint64),
+                ("message", C.c_char * 128)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "submitted", "completed", "failed", "cache_hits", "cache_misses", "evictions", "rebuilds",
+        "bytes_indexed", "bytes_served", "resident_indexes", "resident_bytes", "arena_used",
+        "arena_peak", "arena_bytes", "in_flight", "pending")]
+
+
 _lib = None
 
 
@@ -201,6 +238,15 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_batch_view_get.argtypes = [vp, P(BatchView)]
     lib.gpj_batch_file_layout.argtypes = [vp, u32, P(u64), P(u64), P(u32)]
     lib.gpj_batch_destroy.argtypes = [vp]
+    lib.gpj_server_create.argtypes = [P(ServerConfig), P(vp)]
+    lib.gpj_server_submit.argtypes = [vp, P(Request), P(u64)]
+    lib.gpj_server_poll.argtypes = [vp, P(u64), u32, P(u32), C.c_int64]
+    lib.gpj_server_wait.argtypes = [vp, u64, C.c_int64]
+    lib.gpj_server_response.argtypes = [vp, u64, P(Response)]
+    lib.gpj_server_release.argtypes = [vp, u64]
+    lib.gpj_server_stats_get.argtypes = [vp, P(ServerStats)]
+    lib.gpj_server_clear_cache.argtypes = [vp]
+    lib.gpj_server_destroy.argtypes = [vp]
     for name in EXPORTED_SYMBOLS:
         if name != "gpj_version" and name != "gpj_last_error":
             getattr(lib, name).restype = i32
@@ -400,6 +446,122 @@ class Batch:
         if self._h:
             self._lib.gpj_batch_destroy(self._h)
             self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ServerResult:
+    """A finished request: per-query int32 [lines][slots][2] offset arrays
+    (copied out of the server's pinned arena) and its timestamps (ns,
+    CLOCK_MONOTONIC)."""
+
+    request_id: int
+    status: int
+    message: str
+    cache_hit: bool
+    num_lines: int
+    results: list
+    arrival_ns: int
+    admit_ns: int
+    index_ready_ns: int
+    done_ns: int
+
+    @property
+    def latency_ns(self) -> int:
+        return self.done_ns - self.arrival_ns
+
+
+class Server:
+    """gpj_server: continuous-batching request loop with resident indexes.
+
+    submit(data, queries, file_key) queues a request; queries are
+    (CompiledQuery, base_level, num_levels) triples as for Batch.  `data` is a
+    numpy uint8 array (or anything exposing the buffer protocol) that must stay
+    alive until the request finishes."""
+
+    def __init__(self, device: int = 0, num_slots: int = 32, hbm_budget_bytes: int = 1 << 30,
+                 host_result_bytes: int = 256 << 20, cache_levels: int = 4, flags: int = 0):
+        self._lib = load_library()
+        cfg = ServerConfig(device, num_slots, hbm_budget_bytes, host_result_bytes, cache_levels,
+                           flags)
+        h = C.c_void_p()
+        _check(self._lib.gpj_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, data, queries, file_key: int = 0, arrival_ns: int = 0) -> int:
+        import numpy as np
+        arr = np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data
+        irs = [(C.c_uint8 * max(1, len(c.ir_bytes))).from_buffer_copy(c.ir_bytes or b"\0")
+               for c, _, _ in queries]
+        qa = (BatchQuery * len(queries))(*[
+            BatchQuery(C.addressof(ir), len(c.ir_bytes), c.num_result_slots, base, lv, 0)
+            for (c, base, lv), ir in zip(queries, irs)])
+        req = Request(file_key, arr.ctypes.data if arr.size else None, arr.size,
+                      C.cast(qa, C.c_void_p), len(queries), 0, arrival_ns)
+        rid = C.c_uint64()
+        _check(self._lib.gpj_server_submit(self._h, C.byref(req), C.byref(rid)))
+        self._keep[rid.value] = (arr, [c.num_result_slots for c, _, _ in queries])
+        return rid.value
+
+    def poll(self, capacity: int = 1024, timeout_us: int = 0) -> list:
+        ids = (C.c_uint64 * capacity)()
+        n = C.c_uint32()
+        _check(self._lib.gpj_server_poll(self._h, ids, capacity, C.byref(n), timeout_us))
+        return list(ids[: n.value])
+
+    def wait(self, request_id: int, timeout_us: int = -1) -> None:
+        _check(self._lib.gpj_server_wait(self._h, request_id, timeout_us))
+
+    def response(self, request_id: int, release: bool = True,
+                 copy_results: bool = True) -> ServerResult:
+        import numpy as np
+        r = Response()
+        _check(self._lib.gpj_server_response(self._h, request_id, C.byref(r)))
+        _, slots = self._keep.get(request_id, (None, []))
+        results = []
+        if r.status == GPJ_OK and copy_results:
+            ints = np.ctypeslib.as_array(C.cast(r.h_results, C.POINTER(C.c_int32)),
+                                         shape=(max(r.result_ints, 1),))[: r.result_ints]
+            for q, s in enumerate(slots):
+                off = r.result_offset[q]
+                cnt = r.num_lines * s * 2
+                results.append(ints[off:off + cnt].copy().reshape(r.num_lines, s, 2))
+        out = ServerResult(request_id, r.status, r.message.decode(errors="replace"),
+                           bool(r.cache_hit), r.num_lines, results, r.arrival_ns, r.admit_ns,
+                           r.index_ready_ns, r.done_ns)
+        if release:
+            self.release(request_id)
+        return out
+
+    def release(self, request_id: int) -> None:
+        _check(self._lib.gpj_server_release(self._h, request_id))
+        self._keep.pop(request_id, None)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(self._lib.gpj_server_stats_get(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def clear_cache(self) -> None:
+        _check(self._lib.gpj_server_clear_cache(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.gpj_server_destroy(self._h)
+            self._h = C.c_void_p()
+            self._keep.clear()
 
     def __enter__(self):
         return self

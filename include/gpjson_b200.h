@@ -279,6 +279,114 @@ int gpj_batch_file_layout(const gpj_batch *batch, uint32_t file,
 
 int gpj_batch_destroy(gpj_batch *batch);
 
+/* ---- Serving: continuous batching with resident indexes ------------------
+ *
+ * A server owns one device arena (the HBM budget), one pinned host arena for
+ * results, and num_slots CUDA streams.  A scheduler thread admits submitted
+ * requests in arrival order whenever a slot is free and the request's device
+ * footprint (input copy, bitmaps, newline index, scratch, results) fits the
+ * arena, evicting idle resident indexes least-recently-used first.  Admitted
+ * requests run concurrently, one per stream: H2D copy -> index build ->
+ * queries -> D2H of the results.  Indexes of requests with a nonzero file_key
+ * stay resident after completion, so later requests for the same key and size
+ * skip the copy and the build; a request whose key is being built by another
+ * request waits for that build instead of repeating it.
+ *
+ * The reference answers one Engine::query call at a time and rebuilds every
+ * index (src/gpjson/engine.cpp:131-166); the server has no counterpart there
+ * and runs the same index and query kernels as gpj_index_build_async and
+ * gpj_query_run, so each request's results equal those of that plain path. */
+typedef struct gpj_server gpj_server;
+
+#define GPJ_SERVER_NO_CACHE 1u /* never keep indexes resident */
+#define GPJ_SERVER_SLEEP_POLL 2u /* scheduler sleeps between event polls */
+#define GPJ_SERVER_MAX_QUERIES 8
+
+typedef struct gpj_server_config {
+  int32_t device;
+  int32_t num_slots;           /* requests on the device at once; 0 = 32 */
+  uint64_t hbm_budget_bytes;   /* device arena; 0 = 1 GiB */
+  uint64_t host_result_bytes;  /* pinned result arena; 0 = 256 MiB */
+  int32_t cache_levels;        /* levels built for resident indexes (at least
+                                  each request's own need); 0 = 4 */
+  uint32_t flags;              /* GPJ_SERVER_* */
+  uint32_t reserved[4];
+} gpj_server_config;
+
+/* One request: a file and 1..GPJ_SERVER_MAX_QUERIES compiled queries (the
+ * gpj_batch_query fields: IR, result slots, base level, levels needed).
+ * h_input must stay valid until the request completes; pinned host memory
+ * makes the copy asynchronous.  arrival_ns: the caller's arrival time on
+ * CLOCK_MONOTONIC (0 = the time of submission), the start of the measured
+ * latency.  Files are limited to 2^31 - 1 bytes (int32 offsets). */
+typedef struct gpj_request {
+  uint64_t file_key;           /* resident-index identity; 0 = do not cache */
+  const uint8_t *h_input;
+  uint64_t size_bytes;
+  const gpj_batch_query *queries;
+  uint32_t num_queries;
+  uint32_t reserved;
+  uint64_t arrival_ns;
+} gpj_request;
+
+/* A finished request.  h_results points into the server's pinned arena and
+ * stays valid until gpj_server_release: query q's block starts at int
+ * result_offset[q] and holds int32 [num_lines][slots_q][2] partition-local
+ * [start, end) pairs, -1 where a slot matched nothing (the layout of
+ * gpj_query_run). */
+typedef struct gpj_response {
+  int32_t status;              /* GPJ_OK or the failure's code */
+  int32_t cache_hit;           /* 1: the index was resident (or being built) */
+  uint64_t num_lines;
+  const int32_t *h_results;
+  uint64_t result_ints;
+  uint64_t result_offset[GPJ_SERVER_MAX_QUERIES];
+  uint64_t arrival_ns;
+  uint64_t admit_ns;           /* slot and memory granted */
+  uint64_t index_ready_ns;     /* index available (build done, or cached) */
+  uint64_t done_ns;            /* results on the host */
+  char message[128];           /* failure message, "" on success */
+} gpj_response;
+
+typedef struct gpj_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t cache_hits, cache_misses, evictions, rebuilds;
+  uint64_t bytes_indexed;      /* input bytes copied and indexed */
+  uint64_t bytes_served;       /* input bytes of completed requests */
+  uint64_t resident_indexes, resident_bytes;
+  uint64_t arena_used, arena_peak, arena_bytes;
+  uint64_t in_flight, pending;
+} gpj_server_stats;
+
+int gpj_server_create(const gpj_server_config *config, gpj_server **out);
+
+/* Queues a request (copies the request and its IRs); returns its id. */
+int gpj_server_submit(gpj_server *server, const gpj_request *request, uint64_t *request_id);
+
+/* Waits up to timeout_us (negative: forever) for finished requests not yet
+ * reported by this call and returns up to capacity of their ids. */
+int gpj_server_poll(gpj_server *server, uint64_t *ids, uint32_t capacity, uint32_t *count,
+                    int64_t timeout_us);
+
+/* Waits up to timeout_us (negative: forever) for one request; GPJ_ERR_TIMEOUT
+ * if it is still running. */
+int gpj_server_wait(gpj_server *server, uint64_t request_id, int64_t timeout_us);
+
+/* Response of a finished request (GPJ_ERR_OUT_OF_RANGE if unknown or
+ * released, GPJ_ERR_TIMEOUT if not finished). */
+int gpj_server_response(gpj_server *server, uint64_t request_id, gpj_response *out);
+
+/* Frees a finished request's host results. */
+int gpj_server_release(gpj_server *server, uint64_t request_id);
+
+int gpj_server_stats_get(gpj_server *server, gpj_server_stats *out);
+
+/* Drops every idle resident index. */
+int gpj_server_clear_cache(gpj_server *server);
+
+/* Finishes the requests on the device, fails the queued ones, frees all. */
+int gpj_server_destroy(gpj_server *server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,3 +37,11 @@ def test_no_cpu_path_without_device(gpj):
         pytest.skip("a device is present")
     with pytest.raises(gpj.CudaError, match="no CPU path"):
         gpj.Context(0)
+
+
+def test_server_needs_a_device(gpj):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(gpj.CudaError):
+        gpj.Server(0, hbm_budget_bytes=1 << 20)
