@@ -471,6 +471,7 @@ class ServerResult:
     message: str
     cache_hit: bool
     num_lines: int
+    result_ints: int
     results: list
     arrival_ns: int
     admit_ns: int
@@ -539,7 +540,8 @@ class Server:
                 cnt = r.num_lines * s * 2
                 results.append(ints[off:off + cnt].copy().reshape(r.num_lines, s, 2))
         out = ServerResult(request_id, r.status, r.message.decode(errors="replace"),
-                           bool(r.cache_hit), r.num_lines, results, r.arrival_ns, r.admit_ns,
+                           bool(r.cache_hit), r.num_lines, r.result_ints, results,
+                           r.arrival_ns, r.admit_ns,
                            r.index_ready_ns, r.done_ns)
         if release:
             self.release(request_id)

@@ -1,7 +1,7 @@
 """Benchmark: GpJSON index + query throughput on B200 (one JSON line on stdout).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c1|c0|c2]
+                  [--workload c1|c0|c2|c3|c4]
 
 A step is one pass of the hot path over the workload: the fused structural
 index build of the whole input plus every query of the workload, with the
@@ -12,9 +12,13 @@ queries, D2H of every result array) from pinned memory.
 
 Workloads (seeded synthetic stand-ins for the GpJSON datasets):
   c1  one 1 GiB top-level array of ~2 KiB product records, one element per
-      line; query $[*].categoryPath[1:3].id   (default)
+      line; query $[*].categoryPath[1:3].id
   c0  64 MiB NDJSON of ~2 KiB post records; query $.user.lang
   c2  4 GiB NDJSON post records (deeper nesting); four queries over one index
+  c3  10,000 files (8 GiB) batched in one captured launch chain vs one
+      launch chain per file; the default run appends a 2 s c4 serving trace
+  c4  serving: Poisson request trace through gpj_server, p50/p99 latency,
+      with and without resident-index reuse
 
 Multi-GPU (--gpus N under torchrun): the path has no exchange step, so each
 rank runs an independent replica of the workload ("scaling": "weak") and the
@@ -37,6 +41,10 @@ import time
 from pathlib import Path
 
 import numpy as np
+
+# the serving workload runs up to 32 streams at once: give them their own
+# hardware queues (the default is 8)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -111,9 +119,19 @@ def c3_sizes(seed: int = 3, count: int = 10_000, total: int = 8 << 30,
     return sizes
 
 
-def c3_files(pkg, scale: float = 1.0):
-    """10,000 seeded files (even: NDJSON post records, odd: product arrays)."""
+C3_DESC = ("c3: 10,000 seeded files, log-normal sizes 4 KiB-64 MiB, half NDJSON post records "
+           "($.user.lang), half product arrays ($[*].categoryPath[1:3].id), one captured "
+           "launch chain")
+C3_QUERIES = ["$.user.lang", "$[*].categoryPath[1:3].id"]
+
+
+def c3_files(pkg, scale: float = 1.0, limit_bytes: int | None = None):
+    """10,000 seeded files (even: NDJSON post records, odd: product arrays);
+    with limit_bytes only the leading files up to that many bytes."""
     sizes = c3_sizes(total=int((8 << 30) * scale)) if scale != 1.0 else c3_sizes()
+    if limit_bytes is not None:
+        keep = int(np.searchsorted(np.cumsum(sizes), limit_bytes)) + 1
+        sizes = sizes[:keep]
     dg = pkg.datagen
 
     def make(i):
@@ -124,6 +142,136 @@ def c3_files(pkg, scale: float = 1.0):
 
     with cf.ThreadPoolExecutor(os.cpu_count() or 4) as pool:
         return list(pool.map(make, range(len(sizes))))
+
+
+C4_QUERIES = ["$.user.lang", "$.entities.hashtags[*].text", "$.place.country_code",
+              "$.retweeted_status.user.id"]
+
+
+def c4_trace(pkg, seed: int = 4, rate: float = 2000.0, duration_s: float = 4.0,
+             repeat: float = 0.3, lo: int = 16 << 10, hi: int = 256 << 20,
+             median: int = 256 << 10, sigma: float = 1.5, corpus_bytes: int = 1 << 30):
+    """Serving trace: Poisson arrivals at `rate` for `duration_s`; each request
+    names a file (30% repeats of an earlier file, else a new one whose size is
+    log-normal around `median`, truncated to [lo, hi]) and 1-3 queries of the
+    c2 set.  Files are newline-aligned slices of one seeded NDJSON corpus of
+    post records (depth <= 8).  Returns (corpus, files [(offset, size)],
+    requests [(arrival_s, file, [query indices])])."""
+    dg = pkg.datagen
+    chunk = 64 << 20
+    with cf.ThreadPoolExecutor(os.cpu_count() or 4) as pool:
+        parts = list(pool.map(lambda i: dg.tweets(5_000_000 + i, chunk, deep=True),
+                              range(max(1, corpus_bytes // chunk))))
+    corpus = np.concatenate(parts)
+    nls = np.flatnonzero(corpus == 10)
+    rng = np.random.default_rng(seed)
+    count = int(rate * duration_s)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    hi = min(hi, corpus.size // 2)
+    files, reqs = [], []
+    for t in arrivals:
+        if files and rng.random() < repeat:
+            f = int(rng.integers(len(files)))
+        else:
+            while True:
+                size = int(np.exp(rng.normal(np.log(median), sigma)))
+                if lo <= size <= hi:
+                    break
+            off = int(rng.integers(0, corpus.size - size))
+            k = int(np.searchsorted(nls, off))
+            start = int(nls[k]) + 1 if k < nls.size else 0
+            k2 = int(np.searchsorted(nls, start + size))
+            end = int(nls[min(k2, nls.size - 1)]) + 1
+            files.append((start, max(0, end - start)))
+            f = len(files) - 1
+        nq = int(rng.integers(1, 4))
+        reqs.append((float(t), f, sorted(int(x) for x in rng.choice(4, nq, replace=False))))
+    return corpus, files, reqs
+
+
+def run_serving(args, world, rank, local, duration_s: float | None = None):
+    """c4: the serving loop (gpj_server) fed a Poisson request trace in real
+    time, with and without resident-index reuse, plus the same requests all
+    submitted at once (saturated throughput).  Latency = result on the host
+    minus scheduled arrival."""
+    import torch
+    pkg = entry.package()
+    pkg.load_library()
+    duration = duration_s if duration_s is not None else args.serve_seconds
+    corpus, files, reqs = c4_trace(pkg, duration_s=duration)
+    torch.cuda.set_device(local)
+    pinned = torch.from_numpy(corpus).pin_memory()
+    view = pinned.numpy()
+    comp = [(c, 0, c.max_depth) for c, _ in compile_all(pkg, C4_QUERIES)]
+    budget = min(120 * 10**9, int(torch.cuda.mem_get_info(local)[0] * 0.8))
+
+    def arm(cache: bool, realtime: bool):
+        flags = 0 if cache else pkg.GPJ_SERVER_NO_CACHE
+        srv = pkg.Server(local, num_slots=32, hbm_budget_bytes=budget,
+                         host_result_bytes=2 << 30, cache_levels=4, flags=flags)
+        ids = []
+        t0 = time.monotonic_ns() + 20_000_000
+        for t, f, qs in reqs:
+            off, size = files[f]
+            target = t0 + int(t * 1e9) if realtime else 0
+            if realtime:
+                while time.monotonic_ns() < target:
+                    pass
+            ids.append(srv.submit(view[off:off + size], [comp[q] for q in qs],
+                                  file_key=f + 1, arrival_ns=target))
+        pending = set(ids)
+        while pending:
+            for rid in srv.poll(timeout_us=1_000_000):
+                pending.discard(rid)
+        out = [srv.response(rid, release=False, copy_results=False) for rid in ids]
+        sample = {rid: srv.response(rid, release=False).results for rid in ids[:: max(1, len(ids) // 200)]}
+        st = srv.stats()
+        srv.close()
+        assert all(r.status == 0 for r in out), [r.message for r in out if r.status][:3]
+        lat = np.array([r.done_ns - r.arrival_ns for r in out], np.float64) / 1e6
+        span = (max(r.done_ns for r in out) - min(r.arrival_ns for r in out)) / 1e9
+        served = sum(files[f][1] for _, f, _ in reqs)
+        return {
+            "p50_ms": round(float(np.percentile(lat, 50)), 4),
+            "p99_ms": round(float(np.percentile(lat, 99)), 4),
+            "mean_ms": round(float(lat.mean()), 4),
+            "req_s": round(len(reqs) / span, 1), "gbs": round(served / span / 1e9, 3),
+            "cache_hits": int(st["cache_hits"]), "bytes_indexed": int(st["bytes_indexed"]),
+            "arena_peak_bytes": int(st["arena_peak"]),
+            "index_launches": int(st["cache_misses"] + st["rebuilds"]),
+            "d2h_bytes": int(sum(r.result_ints for r in out)) * 4,
+        }, sample
+
+    # warm-up: a throwaway server runs the first requests (module loading,
+    # first launches of each kernel variant, pinned-page mapping)
+    warm = reqs[:256]
+    srv = pkg.Server(local, num_slots=32, hbm_budget_bytes=min(budget, 8 << 30))
+    for _ in range(3):
+        ids = [srv.submit(view[files[f][0]:files[f][0] + files[f][1]], [comp[q] for q in qs],
+                          file_key=f + 1) for _, f, qs in warm]
+        for rid in ids:
+            srv.wait(rid)
+            srv.release(rid)
+    srv.close()
+
+    rt_reuse, s1 = arm(True, True)
+    rt_plain, s2 = arm(False, True)
+    sat_reuse, _ = arm(True, False)
+    sat_plain, _ = arm(False, False)
+    for rid in s1:
+        for a, b in zip(s1[rid], s2[rid]):
+            assert np.array_equal(a, b), "results differ with and without index reuse"
+    served = sum(files[f][1] for _, f, _ in reqs)
+    return {
+        "workload": f"c4: Poisson {len(reqs) / duration:.0f} req/s for {duration:g} s, "
+                    f"{len(reqs)} requests over {len(files)} files (log-normal 16 KiB-256 MiB, "
+                    "median 256 KiB, 30% repeats), 1-3 of the c2 queries each",
+        "requests": len(reqs), "files": len(files), "bytes_requested": served,
+        "hbm_budget_bytes": budget, "slots": 32,
+        "realtime": {"reuse": rt_reuse, "no_reuse": rt_plain},
+        "saturated": {"reuse": sat_reuse, "no_reuse": sat_plain},
+        "latency": "host-observed: result copied to pinned host memory minus scheduled arrival",
+    }
 
 
 def compile_all(pkg, queries):
@@ -375,8 +523,7 @@ def run_batch(args, world, rank, local):
     pkg = entry.package()
     pkg.load_library()
     files = c3_files(pkg, args.scale)
-    qtext = ["$.user.lang", "$[*].categoryPath[1:3].id"]
-    comp = compile_all(pkg, qtext)
+    comp = compile_all(pkg, C3_QUERIES)
     queries = [(c, base, c.max_depth + base) for c, base in comp]
     buf, offsets = pkg.pack_files([d for d, _ in files])
     total = sum(len(d) for d, _ in files)
@@ -463,10 +610,7 @@ def run_batch(args, world, rank, local):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
-        "config": {"workload": "c3: 10,000 seeded files, log-normal sizes 4 KiB-64 MiB, "
-                               "half NDJSON post records ($.user.lang), half product arrays "
-                               "($[*].categoryPath[1:3].id), one captured launch chain",
-                   "input_bytes": total, "files": len(files), "records": int(v.num_records),
+        "config": {"workload": C3_DESC, "input_bytes": total, "files": len(files), "records": int(v.num_records),
                    "l2": "input larger than L2", "parallelism": f"replicas x{world}",
                    "launch_shape": {"index_threads": v.index_threads,
                                     "query_block": v.query_block, "query_grid": v.query_grid,
@@ -568,12 +712,25 @@ def run_reference(args, world, rank):
     if rank != 0:
         return None
     pkg = entry.package()
-    data, queries, records, desc = workload(args.workload, pkg)
-    comp = compile_all(pkg, queries)
-    levels = max(c.max_depth + base for c, base in comp)
+    if args.workload in ("c3", "c4"):
+        # the leading c3 files (96 MiB) are each step's bounded sample
+        files = c3_files(pkg, limit_bytes=96 << 20)
+        comp = compile_all(pkg, C3_QUERIES)
+        fq = [(c, base, c.max_depth + base) for c, base in comp]
+        queries, desc = C3_QUERIES, C3_DESC
+
+        def step():
+            return cpu_baseline_files(files, comp, fq)
+    else:
+        data, queries, records, desc = workload(args.workload, pkg)
+        comp = compile_all(pkg, queries)
+        levels = max(c.max_depth + base for c, base in comp)
+
+        def step():
+            return cpu_baseline(data, comp, records, levels, budget_s=10.0)
     vals = []
     for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(data, comp, records, levels, budget_s=10.0)
+        cb = step()
         if k >= args.warmup:
             vals.append(cb["value"])
     v = float(np.mean(vals))
@@ -594,7 +751,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c4"])
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="c4: length of the Poisson request trace")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="c3: skip the serving trace that the default run appends")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="c3 only: fraction of the 8 GiB total (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -607,6 +768,27 @@ def main():
         line = run_reference(args, world, rank)
     elif args.workload == "c3":
         line = run_batch(args, world, rank, local)
+        if not args.no_serving:
+            import gc
+            import torch
+            gc.collect()
+            torch.cuda.empty_cache()
+            line["serving"] = run_serving(args, world, rank, local, duration_s=2.0)
+    elif args.workload == "c4":
+        serving = run_serving(args, world, rank, local)
+        sat = serving["saturated"]["reuse"]
+        line = {
+            "metric": METRIC, "value": sat["gbs"], "unit": "GB/s", "n_gpus": world,
+            "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": serving["workload"], "parallelism": f"replicas x{world}",
+                       "l2": "input larger than L2"},
+            "e2e": {"value": sat["gbs"], "unit": "GB/s",
+                    "h2d_bytes_per_step": serving["bytes_requested"],
+                    "d2h_bytes_per_step": sat["d2h_bytes"]},
+            "serving": serving,
+        }
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0 and line is not None:
