@@ -19,86 +19,13 @@
 // string state it starts in, so its look-back descriptor holds the change for
 // both start states; descriptors compose associatively.
 #include "bits.cuh"
+#include "descriptor.cuh"
 #include "indexer.cuh"
 
 #include <cudaTypedefs.h>
 
 namespace gpjb {
 namespace {
-
-// ----------------------------------------------------------------------------
-// Look-back descriptor: one 64-bit word per tile, written with one store.
-//   bits 0-1   status (0 = not ready, 1 = aggregate, 2 = inclusive prefix)
-//   bit  2     string parity: string state after the span if it starts
-//              outside a string (for a constant span: the state after it)
-//   bits 3-10  depth change if the span starts outside a string (mod 256)
-//   bits 11-18 depth change if it starts inside a string (mod 256)
-//   bit  19    constant: the span starts at a file start (state and depth
-//              restart there), so its result does not depend on what came
-//              before; inclusive prefixes are constant too
-//   bits 20-63 newline count (runs on across files)
-// A span is a function from the (string state, depth) entering it to the
-// pair leaving it; composition of such functions is associative, which is
-// what lets one warp fold 128 predecessors per step.
-// ----------------------------------------------------------------------------
-constexpr uint64_t kStatusAgg = 1, kStatusIncl = 2;
-
-struct Agg {
-  uint32_t p;   // string parity (or final state for a constant span)
-  uint32_t d0;  // depth change starting outside a string (mod 256)
-  uint32_t d1;  // depth change starting inside a string (mod 256)
-  uint32_t c;   // 1 = constant span
-  uint64_t n;   // newlines
-};
-
-__device__ __forceinline__ Agg agg_identity() { return Agg{0u, 0u, 0u, 0u, 0ull}; }
-
-// `a` covers the bytes before `b`.
-__device__ __forceinline__ Agg agg_combine(const Agg &a, const Agg &b) {
-  Agg r;
-  r.n = a.n + b.n;
-  if (b.c) {  // b restarts: what came before only adds newlines
-    r.p = b.p;
-    r.d0 = b.d0;
-    r.d1 = b.d1;
-    r.c = 1u;
-  } else if (a.c) {  // constant a: b sees a's final state
-    r.p = a.p ^ b.p;
-    r.d0 = r.d1 = (a.d0 + (a.p ? b.d1 : b.d0)) & 0xFFu;
-    r.c = 1u;
-  } else {
-    r.p = a.p ^ b.p;
-    r.d0 = (a.d0 + (a.p ? b.d1 : b.d0)) & 0xFFu;
-    r.d1 = (a.d1 + (a.p ? b.d0 : b.d1)) & 0xFFu;
-    r.c = 0u;
-  }
-  return r;
-}
-
-__device__ __forceinline__ uint64_t agg_pack(uint64_t status, const Agg &a) {
-  return status | (uint64_t(a.p & 1u) << 2) | (uint64_t(a.d0 & 0xFFu) << 3) |
-         (uint64_t(a.d1 & 0xFFu) << 11) | (uint64_t(a.c & 1u) << 19) | (a.n << 20);
-}
-
-__device__ __forceinline__ Agg agg_unpack(uint64_t v) {
-  Agg a;
-  a.p = uint32_t(v >> 2) & 1u;
-  a.d0 = uint32_t(v >> 3) & 0xFFu;
-  a.d1 = uint32_t(v >> 11) & 0xFFu;
-  a.c = uint32_t(v >> 19) & 1u;
-  a.n = v >> 20;
-  return a;
-}
-
-__device__ __forceinline__ Agg shfl_down_agg(const Agg &a, int off) {
-  Agg r;
-  r.c = __shfl_down_sync(0xFFFFFFFFu, a.c, off);
-  r.p = __shfl_down_sync(0xFFFFFFFFu, a.p, off);
-  r.d0 = __shfl_down_sync(0xFFFFFFFFu, a.d0, off);
-  r.d1 = __shfl_down_sync(0xFFFFFFFFu, a.d1, off);
-  r.n = __shfl_down_sync(0xFFFFFFFFu, a.n, off);
-  return r;
-}
 
 __device__ __forceinline__ uint64_t ld_relaxed(const unsigned long long *p) {
   uint64_t v;
@@ -117,15 +44,27 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 // Warp 0 only.  Publishes the tile's aggregate, then walks back over its
 // predecessors, 128 per round (4 consecutive descriptors per lane, loaded
 // together so one round costs one memory round trip), and returns the tile's
-// exclusive prefix.
+// exclusive prefix.  The fold works on packed descriptors: two shuffles and
+// one branch-free composition per step.
 constexpr int kLookbackPerLane = 4;
+
+__device__ __forceinline__ uint64_t shfl_down_u64(uint64_t v, int off) {
+  const uint32_t lo = __shfl_down_sync(0xFFFFFFFFu, uint32_t(v), off);
+  const uint32_t hi = __shfl_down_sync(0xFFFFFFFFu, uint32_t(v >> 32), off);
+  return (uint64_t(hi) << 32) | lo;
+}
+__device__ __forceinline__ uint64_t shfl_u64(uint64_t v, int src) {
+  const uint32_t lo = __shfl_sync(0xFFFFFFFFu, uint32_t(v), src);
+  const uint32_t hi = __shfl_sync(0xFFFFFFFFu, uint32_t(v >> 32), src);
+  return (uint64_t(hi) << 32) | lo;
+}
 
 __device__ Agg lookback(const IndexLaunch &P, uint32_t tile, const Agg &local) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) return agg_identity();
   if (lane == 0) st_relaxed(&P.tile_state[tile], agg_pack(kStatusAgg, local));
 
-  Agg later = agg_identity();
+  uint64_t later = 0;  // packed identity
   int64_t base = int64_t(tile) - 1;  // newest tile of the window
   for (;;) {
     // lane l covers tiles base - 4l - j, j = 0 (newest) .. 3 (oldest)
@@ -150,34 +89,28 @@ __device__ Agg lookback(const IndexLaunch &P, uint32_t tile, const Agg &local) {
       __nanosleep(polls < 64 ? 20 : 500);
     }
     // fold the lane's descriptors newest-first, stopping at an inclusive one
-    Agg v = agg_identity();
+    uint64_t v = 0;
     bool has_incl = false;
 #pragma unroll
     for (int j = 0; j < kLookbackPerLane; ++j) {
       if (!has_incl) {
-        v = agg_combine(agg_unpack(s[j]), v);
+        v = desc_combine(s[j], v);
         has_incl = (s[j] & 3u) == kStatusIncl;
       }
     }
     const uint32_t incl = __ballot_sync(0xFFFFFFFFu, has_incl);
     const int limit = incl ? (__ffs(incl) - 1) : 31;
-    if (lane > limit) v = agg_identity();
+    if (lane > limit) v = 0;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const Agg o = shfl_down_agg(v, off);  // tiles further back
-      if (lane + off < 32) v = agg_combine(o, v);
+      const uint64_t o = shfl_down_u64(v, off);  // tiles further back
+      if (lane + off < 32) v = desc_combine(o, v);
     }
-    Agg window;
-    window.c = __shfl_sync(0xFFFFFFFFu, v.c, 0);
-    window.p = __shfl_sync(0xFFFFFFFFu, v.p, 0);
-    window.d0 = __shfl_sync(0xFFFFFFFFu, v.d0, 0);
-    window.d1 = __shfl_sync(0xFFFFFFFFu, v.d1, 0);
-    window.n = __shfl_sync(0xFFFFFFFFu, v.n, 0);
-    later = agg_combine(window, later);
+    later = desc_combine(shfl_u64(v, 0), later);
     if (incl) break;
     base -= 32 * kLookbackPerLane;
   }
-  return later;
+  return agg_unpack(later);
 }
 
 // ----------------------------------------------------------------------------
