@@ -2,10 +2,10 @@
 //
 // One launch replaces the reference's whole SharememIndexBuilder chain
 // (src/gpjson/index/sharemem_index_builder.cu:443-458: nine kernels, three
-// thrust scans, four scalar copies, seven passes over the input).  Each CTA
-// takes one 32 KiB tile in ticket order, stages it in shared memory with one
-// TMA tensor load (128-byte swizzle so that every thread reads its own
-// 128-byte row with conflict-free 16-byte loads), and computes per 64-byte
+// thrust scans, four scalar copies, seven passes over the input).  Persistent
+// CTAs take 32 KiB tiles in ticket order, stage each in shared memory with
+// one TMA tensor load (128-byte swizzle so that every thread reads its own
+// 128-byte row with conflict-free 16-byte loads), and compute per 64-byte
 // word:
 //   escape bitmap E   (word-local carry rule, escape-index.cu:29-96)
 //   quote bitmap  Q   = '"' & ~E                     (quote-index.cu:29-95)
@@ -41,8 +41,8 @@ __device__ __forceinline__ void st_relaxed(unsigned long long *p, uint64_t v) {
 // invariant surfaces as an error status on the host instead of a hang.
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-// Warp 0 only.  Publishes the tile's aggregate, then walks back over its
-// predecessors, 128 per round (4 consecutive descriptors per lane, loaded
+// One warp.  Walks back over the predecessors of `tile` (whose own aggregate
+// is already published), 128 per round (4 consecutive descriptors per lane, loaded
 // together so one round costs one memory round trip), and returns the tile's
 // exclusive prefix.  The fold works on packed descriptors: two shuffles and
 // one branch-free composition per step.
@@ -59,10 +59,9 @@ __device__ __forceinline__ uint64_t shfl_u64(uint64_t v, int src) {
   return (uint64_t(hi) << 32) | lo;
 }
 
-__device__ Agg lookback(const IndexLaunch &P, uint32_t tile, const Agg &local) {
+__device__ Agg lookback(const IndexLaunch &P, uint32_t tile) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) return agg_identity();
-  if (lane == 0) st_relaxed(&P.tile_state[tile], agg_pack(kStatusAgg, local));
 
   uint64_t later = 0;  // packed identity
   int64_t base = int64_t(tile) - 1;  // newest tile of the window
@@ -229,117 +228,279 @@ __device__ __forceinline__ uint32_t file_of_tile(const IndexLaunch &P, uint32_t 
   return lo;
 }
 
-// NT threads per CTA, two 64-byte words per thread: a tile is NT * 128 bytes
-// (NT rows of 128 B, one TMA box).
-template <int LMAX, bool kTma, int NT>
-__global__ void __launch_bounds__(NT)
-    index_kernel(const __grid_constant__ CUtensorMap tmap, const IndexLaunch P) {
-  constexpr int NWARPS = NT / 32;
-  constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
-  static_assert(NT % 32 == 0 && NT <= 256, "one TMA box of at most 256 rows per tile");
-  __shared__ __align__(1024) uint8_t s_tile[kTma ? TILE_BYTES : 16];
-  __shared__ __align__(8) uint64_t s_bar;
-  __shared__ uint32_t s_tile_id, s_file_idx;
-  __shared__ IndexFile s_file;
-  __shared__ uint32_t s_halo;
-  __shared__ uint32_t s_last_tp[NWARPS];
-  __shared__ uint32_t s_warp_par[NWARPS];
-  __shared__ uint32_t s_warp_dd[NWARPS];
-  __shared__ uint32_t s_warp_nl[NWARPS];
-  __shared__ uint32_t s_prefix_p, s_prefix_d;
-  __shared__ unsigned long long s_prefix_n;
-
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int warp = tid >> 5;
-
-  if (tid == 0) {
-    const uint32_t t = atomicAdd(P.tile_counter, 1u);
-    s_tile_id = t;
-    if (P.files == nullptr) {
-      s_file_idx = 0;
-      s_file = P.single;
-    } else if (t < P.num_tiles) {
-      const uint32_t f = P.tile_file ? P.tile_file[t] : file_of_tile(P, t);
-      s_file_idx = f;
-      s_file = P.files[f];
-    }
-    if constexpr (kTma) {
-      // the barrier must be initialised before any thread polls it: shared
-      // memory may still hold a barrier of an earlier CTA on this SM
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)));
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
+// ----------------------------------------------------------------------------
+// mbarrier and named-barrier helpers.  Every wait is bounded.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;"
+      " selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// false: gave up after kSpinLimit polls, or the CTA is aborting
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          const volatile uint32_t *abort) {
+  for (uint32_t polls = 0; !mbar_try(bar, parity);) {
+    if (++polls > kSpinLimit || *abort) return false;
   }
-  __syncthreads();
-  const uint32_t tile = s_tile_id;
-  if (tile >= P.num_tiles) return;  // cannot happen with grid == num_tiles
-  const IndexFile F = s_file;
-  const uint32_t file_idx = s_file_idx;
-  const uint32_t ktile = tile - F.first_tile;             // tile within the file
-  const bool file_start = ktile == 0;
-  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;    // tile start within the file
-  const uint64_t valid = min(TILE_BYTES, F.n - byte0);    // bytes of the file in the tile
-  const uint64_t W = (F.n + 63u) / 64u;                   // words of the file
-  const uint8_t *fin = P.in + F.in_off;                   // file bytes
-  const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
+  return true;
+}
 
-  if constexpr (kTma) {
-    if (tid == 0) {
-      const uint32_t bar = smem_u32(&s_bar);
+// Named barrier of the compute warps (the control warp never joins it).
+template <int NT>
+__device__ __forceinline__ void compute_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+}
+// The same barrier, returning the OR of `pred` over the compute threads: a
+// decision every compute thread takes identically.
+template <int NT>
+__device__ __forceinline__ bool compute_sync_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.u32 p, %1, 0; barrier.red.or.pred q, 1, %2, p;"
+      " selp.u32 %0, 1, 0, q; }"
+      : "=r"(r)
+      : "r"(uint32_t(pred)), "n"(NT)
+      : "memory");
+  return r != 0;
+}
+
+// A tile's look-back aggregate from its local scans: string parity, depth
+// sums packed as (change if the tile starts outside a string) | (total << 16),
+// newline count.
+__device__ __forceinline__ Agg tile_aggregate(uint32_t par, uint32_t dd, uint32_t nl,
+                                              bool file_start) {
+  Agg a;
+  a.p = par;
+  a.d0 = dd & 0xFFu;
+  a.d1 = ((dd >> 16) - dd) & 0xFFu;  // total - d0
+  a.c = file_start ? 1u : 0u;
+  if (file_start) a.d1 = a.d0;  // a file starts outside any string
+  a.n = nl;
+  return a;
+}
+
+// ----------------------------------------------------------------------------
+// Persistent pipelined indexer.
+//
+// A CTA is NT compute threads (one 128-byte row of a tile each) plus one
+// control warp.  The compute warps run, for their k-th tile, phase A
+// (classification, escapes, local scans: everything that does not need the
+// file-wide prefix; it ends by publishing the tile's look-back aggregate) and
+// then phase B of tile k-1 (string mask, leveled bitmaps, newline index:
+// everything that does).  The control warp claims the CTA's next tile the
+// moment phase A of the current one ends, stages it into the free one of two
+// shared-memory buffers with a TMA tensor load, and resolves the prefix of
+// the current tile by decoupled look-back while the compute warps run phase
+// B of the previous tile and phase A of the next.
+//
+// Claiming just in time keeps the time from a tile's claim to its aggregate
+// the same for every CTA (phase B of one tile plus phase A of the next), so
+// a tile's predecessors, claimed earlier, have mostly published theirs by
+// the time it looks back.  Tiles are claimed only by running CTAs, in
+// increasing order per CTA, and a CTA's compute warps always work on its
+// smallest unfinished tile, so every wait ends.
+// ----------------------------------------------------------------------------
+constexpr int kStages = 2;
+constexpr uint32_t kEndTile = 0xFFFFFFFFu;
+
+struct StageMeta {  // written by the control warp with each fill
+  uint32_t tile;    // kEndTile: no more tiles for this CTA
+  uint32_t file_idx;
+  uint32_t halo;    // escape carry into the tile
+  uint32_t pad;
+  IndexFile F;
+};
+
+struct TileMeta {  // a tile between its phase A and its phase B
+  uint32_t tile, file_idx;
+  IndexFile F;
+  uint32_t par, dd, nl;  // tile aggregate: string parity, packed depth sums, newlines
+  uint32_t c_in, d_in;   // prefix from the look-back
+  unsigned long long n_in;
+};
+
+template <int NT>
+struct PipeSmem {
+  static constexpr int NW = NT / 32;
+  uint8_t tiles[kStages][NT * 128];
+  unsigned long long full[kStages];
+  unsigned long long agg[2];
+  unsigned long long pref[2];
+  StageMeta stage[kStages];
+  TileMeta tm[2];
+  uint32_t last_tp[NW], warp_par[NW], warp_dd[NW], warp_nl[NW];
+  uint32_t abort;
+};
+
+// One thread's row between phase A and phase B.
+struct RowState {
+  uint64_t op0, cl0, sp0, nl0, op1, cl1, sp1, nl1;
+  uint64_t Sl0, Sl1;
+  uint32_t pex, par0, dd_ex, nl_ex;
+};
+
+// Claims the next tile and stages it into buffer s (warp-collective).
+template <int NT, bool kTma>
+__device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> &sm,
+                                             const CUtensorMap *tmap, int s, bool &ended,
+                                             uint32_t &tile_out) {
+  constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
+  const int lane = threadIdx.x & 31;
+  uint32_t t = 0;
+  if (lane == 0) t = atomicAdd(P.tile_counter, 1u);
+  t = __shfl_sync(0xFFFFFFFFu, t, 0);
+  const uint32_t full = smem_u32(&sm.full[s]);
+  if (t >= P.num_tiles) {
+    ended = true;
+    tile_out = kEndTile;
+    if (lane == 0) {
+      sm.stage[s].tile = kEndTile;
+      mbar_arrive(full);
+    }
+    return;
+  }
+  uint32_t f = 0;
+  IndexFile F;
+  if (P.files == nullptr) {
+    F = P.single;
+  } else {
+    f = P.tile_file ? P.tile_file[t] : file_of_tile(P, t);
+    F = P.files[f];
+  }
+  const uint32_t ktile = t - F.first_tile;
+  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
+  // escape carry: parity of the backslash run ending the word before the
+  // tile, counted inside that word (all 64 bytes read at once)
+  uint32_t halo = 0;
+  if (ktile != 0) {
+    const uint8_t *w = P.in + F.in_off + byte0 - 64u;
+    const uint32_t lo = __ballot_sync(0xFFFFFFFFu, w[lane] != '\\');
+    const uint32_t hi = __ballot_sync(0xFFFFFFFFu, w[32 + lane] != '\\');
+    const uint64_t not_bs = (uint64_t(hi) << 32) | lo;
+    halo = uint32_t(__clzll(static_cast<long long>(not_bs))) & 1u;
+  }
+  if (lane == 0) {
+    sm.stage[s].tile = t;
+    sm.stage[s].file_idx = f;
+    sm.stage[s].halo = halo;
+    sm.stage[s].F = F;
+    if constexpr (kTma) {
+      const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile(
-          "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-          "r"(uint32_t(TILE_BYTES))
-          : "memory");
+      mbar_arrive_tx(full, uint32_t(TILE_BYTES));
       asm volatile(
           "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-          " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(s_tile)),
-          "l"(&tmap), "r"(0), "r"(int32_t(row0)), "r"(bar)
+          " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(sm.tiles[s])),
+          "l"(tmap), "r"(0), "r"(int32_t(row0)), "r"(full)
           : "memory");
+    } else {
+      mbar_arrive(full);
     }
   }
-  // Escape carry into the tile: parity of the backslash run that ends the
-  // previous word of the same file (read backward, at most 64 bytes).
-  if (tid == 0) {
-    uint32_t p = 0;
-    if (!file_start) {
-      for (int k = 1; k <= 64; ++k) {
-        if (fin[byte0 - uint64_t(k)] == '\\') p ^= 1u;
-        else break;
+  tile_out = t;
+}
+
+template <int NT, bool kTma>
+__device__ void control_warp(const IndexLaunch &P, PipeSmem<NT> &sm, const CUtensorMap *tmap) {
+  const int lane = threadIdx.x & 31;
+  const volatile uint32_t *abort = &sm.abort;
+  uint32_t stage_tile[kStages] = {kEndTile, kEndTile};
+  bool ended = false;
+  control_fill<NT, kTma>(P, sm, tmap, 0, ended, stage_tile[0]);
+  uint32_t k = 0;
+  for (;; ++k) {
+    const int s = int(k & 1u);
+    const uint32_t tile = stage_tile[s];
+    if (tile == kEndTile) break;
+    const int j = int(k & 1u);
+    if (!mbar_wait(smem_u32(&sm.agg[j]), (k >> 1) & 1u, abort)) {
+      if (lane == 0) {
+        atomicOr(P.error, kErrPipelineTimeout);
+        sm.abort = 1;
+      }
+      break;
+    }
+    // phase A of tile k is done: claim and stage tile k+1 at once (the
+    // other buffer was read by phase A of tile k-1), then resolve k's prefix
+    if (!ended) control_fill<NT, kTma>(P, sm, tmap, s ^ 1, ended, stage_tile[s ^ 1]);
+    stage_tile[s] = kEndTile;
+
+    TileMeta &tm = sm.tm[j];
+    const IndexFile F = tm.F;
+    const bool file_start = tile == F.first_tile;
+    const Agg local = tile_aggregate(tm.par, tm.dd, tm.nl, file_start);
+    const Agg prefix = lookback(P, tile);
+    if (lane == 0) {
+      const Agg incl = agg_combine(prefix, local);
+      st_relaxed(&P.tile_state[tile], agg_pack(kStatusIncl, incl));
+      tm.c_in = file_start ? 0u : prefix.p;
+      tm.d_in = file_start ? 0u : prefix.d0;
+      tm.n_in = prefix.n;
+      if (P.files == nullptr && tile + 1 == P.num_tiles) {
+        P.summary[0] = incl.n + 1u;  // lines = newlines + 1
+        P.summary[1] = incl.p;
+        P.summary[2] = uint64_t(int64_t(int8_t(uint8_t(incl.d0 - 1u))));
+      }
+      if (file_start && prefix.n + tm.file_idx < P.nl_cap) P.NL[prefix.n + tm.file_idx] = 0;
+      mbar_arrive(smem_u32(&sm.pref[j]));
+    }
+    __syncwarp();
+  }
+  // no TMA may still be writing this CTA's shared memory when it exits: a
+  // staged tile not yet consumed is the one of iteration k (buffer k & 1) or
+  // k + 1 (the other buffer)
+  if constexpr (kTma) {
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) {
+      if (stage_tile[s] == kEndTile) continue;
+      const uint32_t kk = (uint32_t(s) == (k & 1u)) ? k : k + 1u;
+      for (uint32_t polls = 0; !mbar_try(smem_u32(&sm.full[s]), (kk >> 1) & 1u) &&
+                               polls < kSpinLimit;
+           ++polls) {
       }
     }
-    s_halo = p;
   }
+}
 
-  // Thread `tid` owns tile row `tid`: bytes [128 tid, 128 tid + 128) of the
-  // tile, i.e. words lw0 and lw0 + 1 of the file.
+template <int LMAX, bool kTma, int NT>
+__device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, int s, uint32_t k,
+                                        RowState &st) {
+  constexpr int NWARPS = NT / 32;
+  constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const StageMeta &m = sm.stage[s];
+  const uint32_t tile = m.tile;
+  const IndexFile F = m.F;
+  const uint32_t ktile = tile - F.first_tile;
+  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
+  const uint64_t valid = min(TILE_BYTES, F.n - byte0);
+  const uint8_t *fin = P.in + F.in_off;
+  const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
   const uint64_t row_byte = uint64_t(tid) * 128u;
   const uint64_t lw0 = byte0 / 64u + 2u * uint64_t(tid);
-  const bool row_in_smem = kTma && row_byte + 128u <= valid &&
-                           row0 + tid < int64_t(P.full_rows);
-  if constexpr (kTma) {
-    const uint32_t bar = smem_u32(&s_bar);
-    uint32_t done = 0, polls = 0;
-    while (!done) {
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;"
-          " selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(bar)
-          : "memory");
-      if (!done && ++polls > kSpinLimit) {
-        atomicOr(P.error, kErrTmaTimeout);
-        break;
-      }
-    }
-  }
+  const bool row_in_smem =
+      kTma && row_byte + 128u <= valid && row0 + tid < int64_t(P.full_rows);
   uint32_t r[16];
   WordClasses c0, c1;
   if (row_in_smem) {
-    load_word_smem(s_tile, tid, 0, r);
+    load_word_smem(sm.tiles[s], tid, 0, r);
     c0 = classify64(r);
-    load_word_smem(s_tile, tid, 1, r);
+    load_word_smem(sm.tiles[s], tid, 1, r);
     c1 = classify64(r);
   } else {
     // rows past the end of the file read as zero bytes (no class)
@@ -350,17 +511,12 @@ __global__ void __launch_bounds__(NT)
     load_word_global(rp, lim, 64, r);
     c1 = classify64(r);
   }
-
-  // --- escape carries between words --------------------------------------
   const uint32_t tp0 = trailing_escape_parity(c0.bs);
   const uint32_t tp1 = trailing_escape_parity(c1.bs);
-  if (lane == 31) s_last_tp[warp] = tp1;
-  __syncthreads();  // (1) s_last_tp, s_halo; every thread is past the barrier wait
-  if constexpr (kTma) {
-    if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&s_bar)));
-  }
+  if (lane == 31) sm.last_tp[warp] = tp1;
+  compute_sync<NT>();  // (1) last_tp; every row of buffer s has been read
   uint32_t cin0 = __shfl_up_sync(0xFFFFFFFFu, tp1, 1);
-  if (lane == 0) cin0 = (warp == 0) ? s_halo : s_last_tp[warp - 1];
+  if (lane == 0) cin0 = (warp == 0) ? m.halo : sm.last_tp[warp - 1];
 
   const uint64_t E0 = escaped_bits(c0.bs, cin0);
   const uint64_t E1 = escaped_bits(c1.bs, tp0);
@@ -370,6 +526,11 @@ __global__ void __launch_bounds__(NT)
   const uint64_t Sl1 = prefix_xor(Q1);
   const uint32_t par0 = uint32_t(popc64(Q0)) & 1u;
   const uint32_t par1 = uint32_t(popc64(Q1)) & 1u;
+  if (P.E != nullptr) {
+    const uint64_t W = (F.n + 63u) / 64u;
+    store2(P.E + F.s_off, lw0, W, E0 & valid_mask(lw0, F.n), E1 & valid_mask(lw0 + 1, F.n));
+    store2(P.Q + F.s_off, lw0, W, Q0, Q1);
+  }
 
   // depth change of each word if it starts outside a string, and in total
   const int d00 = popc64(c0.op & ~Sl0) - popc64(c0.cl & ~Sl0);
@@ -381,23 +542,22 @@ __global__ void __launch_bounds__(NT)
   const uint32_t thr_par = par0 ^ par1;
   const uint32_t thr_nl = uint32_t(popc64(c0.nl) + popc64(c1.nl));
 
-  // --- tile-local exclusive scans ------------------------------------------
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t par_ballot = __ballot_sync(0xFFFFFFFFu, thr_par);
   uint32_t pex = uint32_t(__popc(par_ballot & lt_mask)) & 1u;
-  if (lane == 0) s_warp_par[warp] = uint32_t(__popc(par_ballot)) & 1u;
-  __syncthreads();  // (2)
-  for (int w = 0; w < warp; ++w) pex ^= s_warp_par[w];
+  if (lane == 0) sm.warp_par[warp] = uint32_t(__popc(par_ballot)) & 1u;
+  compute_sync<NT>();  // (2)
   uint32_t tile_par = 0;
 #pragma unroll
-  for (int w = 0; w < NWARPS; ++w) tile_par ^= s_warp_par[w];
-
+  for (int w = 0; w < NWARPS; ++w) {
+    if (w < warp) pex ^= sm.warp_par[w];
+    tile_par ^= sm.warp_par[w];
+  }
   // depth changes are only needed mod 256: two 16-bit lanes cannot overflow
   // over at most 256 threads (256 * 255 < 65536)
   const int dt0 = pex ? (thr_t - thr_d0) : thr_d0;
-  uint32_t dd = (uint32_t(dt0) & 0xFFu) | ((uint32_t(thr_t) & 0xFFu) << 16);
-  uint32_t nl = thr_nl;
-  uint32_t dd_inc = dd, nl_inc = nl;
+  const uint32_t dd = (uint32_t(dt0) & 0xFFu) | ((uint32_t(thr_t) & 0xFFu) << 16);
+  uint32_t dd_inc = dd, nl_inc = thr_nl;
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
     const uint32_t a = __shfl_up_sync(0xFFFFFFFFu, dd_inc, off);
@@ -408,107 +568,190 @@ __global__ void __launch_bounds__(NT)
     }
   }
   if (lane == 31) {
-    s_warp_dd[warp] = dd_inc;
-    s_warp_nl[warp] = nl_inc;
+    sm.warp_dd[warp] = dd_inc;
+    sm.warp_nl[warp] = nl_inc;
   }
-  __syncthreads();  // (3)
-  uint32_t dd_ex = dd_inc - dd, nl_ex = nl_inc - nl;
+  compute_sync<NT>();  // (3)
+  uint32_t dd_ex = dd_inc - dd, nl_ex = nl_inc - thr_nl;
   uint32_t tile_dd = 0, tile_nl = 0;
 #pragma unroll
   for (int w = 0; w < NWARPS; ++w) {
     if (w < warp) {
-      dd_ex += s_warp_dd[w];
-      nl_ex += s_warp_nl[w];
+      dd_ex += sm.warp_dd[w];
+      nl_ex += sm.warp_nl[w];
     }
-    tile_dd += s_warp_dd[w];
-    tile_nl += s_warp_nl[w];
+    tile_dd += sm.warp_dd[w];
+    tile_nl += sm.warp_nl[w];
   }
-
-  // --- decoupled look-back --------------------------------------------------
-  if (warp == 0) {
-    Agg local;
-    local.p = tile_par;
-    local.d0 = tile_dd & 0xFFu;
-    local.d1 = ((tile_dd >> 16) - tile_dd) & 0xFFu;  // total - d0
-    local.c = file_start ? 1u : 0u;
-    if (file_start) local.d1 = local.d0;  // a file starts outside any string
-    local.n = tile_nl;
-    const Agg prefix = lookback(P, tile, local);
-    if (lane == 0) {
-      const Agg incl = agg_combine(prefix, local);
-      st_relaxed(&P.tile_state[tile], agg_pack(kStatusIncl, incl));
-      // a file start ignores the string state and depth of what precedes it
-      s_prefix_p = file_start ? 0u : prefix.p;
-      s_prefix_d = file_start ? 0u : prefix.d0;
-      s_prefix_n = prefix.n;
-      if (P.files == nullptr && tile + 1 == P.num_tiles) {
-        P.summary[0] = incl.n + 1u;  // lines = newlines + 1
-        P.summary[1] = incl.p;
-        P.summary[2] = uint64_t(int64_t(int8_t(uint8_t(incl.d0 - 1u))));
-      }
-      // newline index of the file starts with 0, at (newlines before it) + f
-      if (file_start && prefix.n + file_idx < P.nl_cap) P.NL[prefix.n + file_idx] = 0;
-    }
+  if (tid == 0) {
+    // publish the aggregate at once: look-backs of later tiles wait for it
+    if (tile != 0)
+      st_relaxed(&P.tile_state[tile],
+                 agg_pack(kStatusAgg, tile_aggregate(tile_par, tile_dd, tile_nl, ktile == 0)));
+    TileMeta &tm = sm.tm[k & 1u];
+    tm.tile = tile;
+    tm.file_idx = m.file_idx;
+    tm.F = F;
+    tm.par = tile_par;
+    tm.dd = tile_dd;
+    tm.nl = tile_nl;
+    mbar_arrive(smem_u32(&sm.agg[k & 1u]));
   }
-  __syncthreads();  // (4)
-  const uint32_t c_in = s_prefix_p;
-  const uint32_t d_in = s_prefix_d;
-  const uint64_t nl_base = s_prefix_n + nl_ex + file_idx;  // slot of my first newline - 1
+  st.op0 = c0.op;
+  st.cl0 = c0.cl;
+  st.sp0 = c0.sp;
+  st.nl0 = c0.nl;
+  st.op1 = c1.op;
+  st.cl1 = c1.cl;
+  st.sp1 = c1.sp;
+  st.nl1 = c1.nl;
+  st.Sl0 = Sl0;
+  st.Sl1 = Sl1;
+  st.pex = pex;
+  st.par0 = par0;
+  st.dd_ex = dd_ex;
+  st.nl_ex = nl_ex;
+}
 
-  // --- outputs ----------------------------------------------------------------
-  const uint32_t car0 = c_in ^ pex;
-  const uint32_t car1 = car0 ^ par0;
-  const uint64_t S0 = Sl0 ^ (car0 ? ~0ull : 0ull);
-  const uint64_t S1 = Sl1 ^ (car1 ? ~0ull : 0ull);
-  const uint32_t a_ex = dd_ex & 0xFFu, t_ex = (dd_ex >> 16) & 0xFFu;
+template <int LMAX, int NT>
+__device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm, uint32_t k,
+                                        const RowState &st) {
+  constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
+  const int tid = threadIdx.x;
+  const int j = int(k & 1u);
+  if (!mbar_wait(smem_u32(&sm.pref[j]), (k >> 1) & 1u, &sm.abort)) {
+    atomicOr(P.error, kErrPipelineTimeout);
+    sm.abort = 1;
+    return;
+  }
+  const TileMeta &tm = sm.tm[j];
+  const IndexFile F = tm.F;
+  const uint32_t ktile = tm.tile - F.first_tile;
+  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
+  const uint64_t W = (F.n + 63u) / 64u;
+  const uint64_t lw0 = byte0 / 64u + 2u * uint64_t(tid);
+  const uint32_t c_in = tm.c_in, d_in = tm.d_in;
+  const uint64_t nl_base = tm.n_in + st.nl_ex + tm.file_idx;  // slot of my first newline - 1
+
+  const uint32_t car0 = c_in ^ st.pex;
+  const uint32_t car1 = car0 ^ st.par0;
+  const uint64_t S0 = st.Sl0 ^ (car0 ? ~0ull : 0ull);
+  const uint64_t S1 = st.Sl1 ^ (car1 ? ~0ull : 0ull);
+  const uint32_t a_ex = st.dd_ex & 0xFFu, t_ex = (st.dd_ex >> 16) & 0xFFu;
   const int depth0 = int(int8_t(uint8_t(d_in - 1u + (c_in ? (t_ex - a_ex) : a_ex))));
 
   store2(P.S + F.s_off, lw0, W, S0, S1);
-  if (P.E != nullptr) {
-    store2(P.E + F.s_off, lw0, W, E0 & valid_mask(lw0, F.n), E1 & valid_mask(lw0 + 1, F.n));
-    store2(P.Q + F.s_off, lw0, W, Q0, Q1);
-  }
-
   if (F.levels > 0) {
     uint64_t lb0[LMAX], lb1[LMAX];
     const int depth1 =
-        leveled_word<LMAX>(c0.op & ~S0, c0.cl & ~S0, c0.sp & ~S0, depth0, lb0);
-    leveled_word<LMAX>(c1.op & ~S1, c1.cl & ~S1, c1.sp & ~S1, depth1, lb1);
+        leveled_word<LMAX>(st.op0 & ~S0, st.cl0 & ~S0, st.sp0 & ~S0, depth0, lb0);
+    leveled_word<LMAX>(st.op1 & ~S1, st.cl1 & ~S1, st.sp1 & ~S1, depth1, lb1);
 #pragma unroll
     for (int l = 0; l < LMAX; ++l) {
       if (l < F.levels) store2(P.LB + F.lb_off + uint64_t(l) * W, lw0, W, lb0[l], lb1[l]);
     }
   }
-
   // newline offsets (every '\n' counts, strings or not), file-local
-  uint64_t k = nl_base;
-  uint64_t m = c0.nl;
+  uint64_t kk = nl_base;
+  uint64_t m = st.nl0;
   while (m) {
     const int b = __ffsll(static_cast<long long>(m)) - 1;
-    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t(lw0 * 64u + uint64_t(b));
-    ++k;
+    if (kk + 1 < P.nl_cap) P.NL[kk + 1] = int64_t(lw0 * 64u + uint64_t(b));
+    ++kk;
     m &= m - 1;
   }
-  m = c1.nl;
+  m = st.nl1;
   while (m) {
     const int b = __ffsll(static_cast<long long>(m)) - 1;
-    if (k + 1 < P.nl_cap) P.NL[k + 1] = int64_t((lw0 + 1) * 64u + uint64_t(b));
-    ++k;
+    if (kk + 1 < P.nl_cap) P.NL[kk + 1] = int64_t((lw0 + 1) * 64u + uint64_t(b));
+    ++kk;
     m &= m - 1;
   }
+}
+
+template <int LMAX, bool kTma, int NT>
+__global__ void __launch_bounds__(NT + 32, LMAX > 8 ? 1 : (NT <= 128 ? 4 : 2))
+    index_kernel(const __grid_constant__ CUtensorMap tmap, const IndexLaunch P) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // the 128-byte-swizzled TMA destinations need 1024-byte alignment
+  uint8_t *smem_base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  PipeSmem<NT> &sm = *reinterpret_cast<PipeSmem<NT> *>(smem_base);
+  const int tid = threadIdx.x;
+  if (tid == NT) {
+    // barriers must be initialised before anyone polls them: shared memory
+    // may still hold barriers of an earlier CTA on this SM
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(smem_u32(&sm.full[s]), 1);
+      sm.stage[s].tile = kEndTile;
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      mbar_init(smem_u32(&sm.agg[j]), 1);
+      mbar_init(smem_u32(&sm.pref[j]), 1);
+    }
+    sm.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid >= NT) {
+    control_warp<NT, kTma>(P, sm, &tmap);
+    return;
+  }
+  RowState prev{};
+  uint32_t k = 0;
+  for (;; ++k) {
+    const int s = int(k & 1u);
+    bool stop = !mbar_wait(smem_u32(&sm.full[s]), (k >> 1) & 1u, &sm.abort);
+    if (stop) {
+      atomicOr(P.error, kErrTmaTimeout);
+      sm.abort = 1;
+    }
+    // one decision for all compute threads: buffer s is read only when every
+    // one of them saw it filled
+    stop = compute_sync_or<NT>(stop || *static_cast<volatile uint32_t *>(&sm.abort) != 0 ||
+                               sm.stage[s].tile == kEndTile);
+    if (stop) break;
+    RowState cur;
+    phase_a<LMAX, kTma, NT>(P, sm, s, k, cur);
+    if (k > 0) phase_b<LMAX, NT>(P, sm, k - 1, prev);
+    prev = cur;
+  }
+  if (k > 0 && !*static_cast<volatile uint32_t *>(&sm.abort))
+    phase_b<LMAX, NT>(P, sm, k - 1, prev);
+}
+
+template <int LMAX, bool kTma, int NT>
+cudaError_t launch_kernel(const IndexLaunch &L, const CUtensorMap &map, cudaStream_t stream) {
+  auto kernel = index_kernel<LMAX, kTma, NT>;
+  constexpr size_t smem = sizeof(PipeSmem<NT>) + 1024;  // + alignment slack
+  static int grid_per_device[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (grid_per_device[dev] == 0) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT + 32, smem);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    grid_per_device[dev] = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }
+  const uint32_t grid = min(L.num_tiles, uint32_t(grid_per_device[dev]));
+  kernel<<<grid, NT + 32, smem, stream>>>(map, L);
+  return cudaGetLastError();
 }
 
 template <int LMAX, int NT>
 cudaError_t launch_levels(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
                           cudaStream_t stream) {
-  const dim3 grid(L.num_tiles), block(NT);
-  if (use_tma) {
-    index_kernel<LMAX, true, NT><<<grid, block, 0, stream>>>(*map, L);
-  } else {
-    CUtensorMap dummy{};
-    index_kernel<LMAX, false, NT><<<grid, block, 0, stream>>>(dummy, L);
-  }
-  return cudaGetLastError();
+  if (use_tma) return launch_kernel<LMAX, true, NT>(L, *map, stream);
+  CUtensorMap dummy{};
+  return launch_kernel<LMAX, false, NT>(L, dummy, stream);
 }
 
 template <int NT>

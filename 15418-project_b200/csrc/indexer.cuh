@@ -57,6 +57,7 @@ struct IndexLaunch {
 enum : unsigned int {
   kErrLookbackTimeout = 1u,
   kErrTmaTimeout = 2u,
+  kErrPipelineTimeout = 4u,  // a wait between the control and compute warps
 };
 
 inline uint64_t index_num_tiles(uint64_t n) {
