@@ -408,6 +408,14 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
           " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(sm.tiles[s])),
           "l"(tmap), "r"(0), "r"(int32_t(row0)), "r"(full)
           : "memory");
+      // Every CTA claims about one tile per iteration, so the tiles claimed
+      // one iteration from now lie about gridDim.x tiles ahead: pull that
+      // stretch of the input into L2 so their TMA loads hit it.
+      const uint64_t pf = F.in_off + byte0 + uint64_t(gridDim.x) * TILE_BYTES;
+      if (pf + TILE_BYTES <= P.full_rows * 128u)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.in + pf),
+                     "r"(uint32_t(TILE_BYTES))
+                     : "memory");
     } else {
       mbar_arrive(full);
     }
