@@ -26,41 +26,55 @@ enum : uint8_t {
 
 // Last bitmap word read, per thread: consecutive searches of a record mostly
 // start in the word the previous search ended in.
+template <typename Pos>
 struct WordCache {
   const uint64_t *bm = nullptr;
-  int64_t idx = -1;
+  Pos idx = -1;
   uint64_t val = 0;
 };
 
+template <typename Pos>
 struct Rec {
   const uint8_t *in;
-  int64_t n;
+  Pos n;
   const uint64_t *S;
   const uint64_t *LB;
-  int64_t W;
+  Pos W;
   const uint8_t *ir;  // shared memory
   int ir_len;
   int base;    // bitmap level of query level 0
   int levels;  // levels present in LB
 };
 
+// Per-thread interpreter state indexed by query level, in shared memory
+// (slot [level * stride + thread]): the end of each open level and the
+// current array index at it.  `nlev` levels are held: the deepest level the
+// IR can reach (query_ir_levels), at most kMaxQueryLevels.
+template <typename Pos>
+struct LevelState {
+  Pos *end;
+  int32_t *index;
+  int stride, nlev;
+  __device__ __forceinline__ Pos &level_end(int l) const { return end[l * stride]; }
+  __device__ __forceinline__ int32_t &curr_index(int l) const { return index[l * stride]; }
+};
+
 // The reference reads file[] unguarded; well-formed JSON never leaves the
 // partition.  Out-of-range reads return 0 here.
-__device__ __forceinline__ uint8_t at(const Rec &c, int64_t i) {
+template <typename Pos>
+__device__ __forceinline__ uint8_t at(const Rec<Pos> &c, Pos i) {
   return (i >= 0 && i < c.n) ? c.in[i] : uint8_t(0);
 }
-__device__ __forceinline__ uint64_t word_at(const uint64_t *bm, int64_t W,
-                                            int64_t i) {
-  return (i >= 0 && i < W) ? bm[i] : 0ull;
-}
-__device__ __forceinline__ uint8_t ir_at(const Rec &c, int64_t i) {
+template <typename Pos>
+__device__ __forceinline__ uint8_t ir_at(const Rec<Pos> &c, int i) {
   return (i >= 0 && i < c.ir_len) ? c.ir[i] : uint8_t(0);
 }
 
-__device__ __forceinline__ uint64_t cached_word(WordCache &wc, const uint64_t *bm, int64_t W,
-                                                int64_t i) {
+template <typename Pos>
+__device__ __forceinline__ uint64_t cached_word(WordCache<Pos> &wc, const uint64_t *bm, Pos W,
+                                                Pos i) {
   if (wc.bm == bm && wc.idx == i) return wc.val;
-  const uint64_t v = word_at(bm, W, i);
+  const uint64_t v = (i >= 0 && i < W) ? bm[i] : 0ull;
   wc.bm = bm;
   wc.idx = i;
   wc.val = v;
@@ -72,15 +86,16 @@ __device__ __forceinline__ uint64_t mask_through_bit(int b) {
 }
 
 // query.cu:39-77
-__device__ int64_t prev_bit(WordCache &wc, const uint64_t *bm, int64_t W, int64_t min_index,
-                            int64_t line_index) {
+template <typename Pos>
+__device__ Pos prev_bit(WordCache<Pos> &wc, const uint64_t *bm, Pos W, Pos min_index,
+                        Pos line_index) {
   if (line_index < min_index) return -1;
-  int64_t wi = line_index >> 6;
-  int64_t base = wi * 64;
+  Pos wi = line_index >> 6;
+  Pos base = wi * 64;
   uint64_t word = cached_word(wc, bm, W, wi) & mask_through_bit(int(line_index - base));
   while (base + 63 >= min_index) {
     uint64_t cand = word;
-    const int64_t first = min_index - base;
+    const Pos first = min_index - base;
     if (first > 0) cand &= ~mask_through_bit(int(first - 1));
     if (cand != 0) return base + 63 - __clzll(static_cast<long long>(cand));
     if (wi == 0) break;
@@ -93,18 +108,19 @@ __device__ int64_t prev_bit(WordCache &wc, const uint64_t *bm, int64_t W, int64_
 }
 
 // query.cu:79-115
-__device__ int64_t next_struct(const Rec &c, WordCache &wc, int64_t level_end,
-                               int64_t line_index, int level) {
+template <typename Pos>
+__device__ Pos next_struct(const Rec<Pos> &c, WordCache<Pos> &wc, Pos level_end, Pos line_index,
+                           int level) {
   if (line_index >= level_end) return level_end;
   // a level the index does not hold has no structural characters
   if (level + c.base < 0 || level + c.base >= c.levels) return level_end;
   const uint64_t *lvl = c.LB + uint64_t(c.W) * uint64_t(level + c.base);
-  int64_t wi = line_index >> 6;
-  int64_t base = wi * 64;
+  Pos wi = line_index >> 6;
+  Pos base = wi * 64;
   uint64_t word = cached_word(wc, lvl, c.W, wi) & (~0ull << (line_index - base));
   while (base <= level_end) {
     uint64_t cand = word;
-    const int64_t last = level_end - base;
+    const Pos last = level_end - base;
     if (last < 63) cand &= mask_through_bit(int(last));
     if (cand != 0) return base + __ffsll(static_cast<long long>(cand)) - 1;
     ++wi;
@@ -116,19 +132,21 @@ __device__ int64_t next_struct(const Rec &c, WordCache &wc, int64_t level_end,
 }
 
 // query.cu:117-128
-__device__ int64_t prev_struct(const Rec &c, WordCache &wc, int64_t level_start,
-                               int64_t line_index, int level) {
+template <typename Pos>
+__device__ Pos prev_struct(const Rec<Pos> &c, WordCache<Pos> &wc, Pos level_start, Pos line_index,
+                           int level) {
   if (line_index <= level_start) return level_start;
   if (level + c.base < 0 || level + c.base >= c.levels) return level_start;
   const uint64_t *lvl = c.LB + uint64_t(c.W) * uint64_t(level + c.base);
-  const int64_t s = prev_bit(wc, lvl, c.W, level_start, line_index);
+  const Pos s = prev_bit(wc, lvl, c.W, level_start, line_index);
   return s == -1 ? level_start : s;
 }
 
 // query.cu:130-140 (LEB128).  Unsigned arithmetic reinterpreted as int, as
 // the reference's int result wraps; an operand longer than five bytes (never
 // produced by the compiler) reads as -1.
-__device__ int read_varint(const Rec &c, int64_t &pos) {
+template <typename Pos>
+__device__ int read_varint(const Rec<Pos> &c, int &pos) {
   uint32_t value = 0, byte = 0;
   int shift = 0;
   while (((byte = ir_at(c, pos++)) & 0x80u) != 0) {
@@ -139,41 +157,41 @@ __device__ int read_varint(const Rec &c, int64_t &pos) {
   return int(value | (byte << shift));
 }
 
-template <typename OutT>
-__device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
-                           int num_results, OutT *out) {
+template <typename Pos, typename OutT>
+__device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line_start,
+                           Pos line_end, int num_results, OutT *out) {
   if (line_start < 0 || line_start >= c.n || line_end < 0) return;
   if (line_end >= c.n) line_end = c.n - 1;
   while (line_end > line_start && at(c, line_end) != '}') --line_end;
   while (line_start < line_end && at(c, line_start) != '{') ++line_start;
   if (line_start == line_end) return;
 
-  int64_t line_index = line_start;
+  Pos line_index = line_start;
   int level = 0;
-  int64_t qp = 0;
+  int qp = 0;
   // Step bound of one search loop.  On well-formed JSON every step lands on a
   // new structural character of the record, so the bound is never reached;
   // on malformed input the reference's loops can revisit the same character
   // forever, and the record is abandoned instead.
-  const int64_t max_steps = (line_end - line_start) + 2;
-  int64_t steps = 0;
-  WordCache lbc, sc;  // leveled-bitmap and string-mask words
-  int64_t level_end[kMaxQueryLevels];
-  level_end[0] = line_end;
-#pragma unroll
-  for (int i = 1; i < kMaxQueryLevels; ++i) level_end[i] = -1;
-  int64_t marked_pos[kMaxQueryLevels];
+  const Pos max_steps = (line_end - line_start) + 2;
+  Pos steps = 0;
+  WordCache<Pos> lbc, sc;  // leveled-bitmap and string-mask words
+  L.level_end(0) = line_end;
+  L.curr_index(0) = -1;
+  for (int i = 1; i < L.nlev; ++i) {
+    L.level_end(i) = -1;
+    L.curr_index(i) = -1;
+  }
+  // marks belong to filter expressions only: rare, kept in local memory
+  Pos marked_pos[kMaxQueryLevels];
   int marked_level[kMaxQueryLevels];
   int marked = -1;
   int stored = 0;
-  int64_t key_pos = 0;
+  int key_pos = 0;
   int key_len = 0;
   int target = 0;
-  int64_t curr_index[kMaxQueryLevels];
-#pragma unroll
-  for (int i = 0; i < kMaxQueryLevels; ++i) curr_index[i] = -1;
 
-#define LEVEL_OK(l) ((l) >= 0 && (l) < kMaxQueryLevels)
+#define LEVEL_OK(l) ((l) >= 0 && (l) < L.nlev)
   for (;;) {
     const uint8_t op = ir_at(c, qp++);
     switch (op) {
@@ -181,8 +199,9 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       return;
     case OP_STORE_RESULT: {
       if (!LEVEL_OK(level)) return;
-      int64_t end_str = level_end[level];
-      while (at(c, line_index) == ' ' && line_index < level_end[level]) ++line_index;
+      const Pos lend = L.level_end(level);
+      Pos end_str = lend;
+      while (at(c, line_index) == ' ' && line_index < lend) ++line_index;
       while (end_str > line_index && at(c, end_str - 1) == ' ') --end_str;
       if (stored < num_results) {
         out[2 * stored] = OutT(line_index);
@@ -193,39 +212,41 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
     }
     case OP_MOVE_UP:
       if (!LEVEL_OK(level)) return;
-      line_index = level_end[level];
-      level_end[level] = -1;
+      line_index = L.level_end(level);
+      L.level_end(level) = -1;
       --level;
       break;
     case OP_MOVE_DOWN:
       ++level;
       if (!LEVEL_OK(level) || level < 1) return;
-      if (level_end[level] == -1) {
-        level_end[level] = next_struct(c, lbc, level_end[level - 1], line_index + 1, level - 1);
+      if (L.level_end(level) == -1) {
+        L.level_end(level) =
+            next_struct(c, lbc, L.level_end(level - 1), Pos(line_index + 1), level - 1);
         while (at(c, line_index) == ' ') ++line_index;
       }
       break;
-    case OP_MOVE_TO_KEY:
+    case OP_MOVE_TO_KEY: {
       key_len = read_varint(c, qp);
       key_pos = qp;
       qp += key_len;
       if (key_len < 0 || !LEVEL_OK(level)) return;
       if (at(c, line_index) != '{') return;
+      const Pos lend = L.level_end(level);
       steps = 0;
       for (;;) {
         if (++steps > max_steps) return;
         ++line_index;
-        line_index = next_struct(c, lbc, level_end[level], line_index, level);
+        line_index = next_struct(c, lbc, lend, line_index, level);
         if (at(c, line_index) == ':') {
-          const int64_t string_end = prev_bit(sc, c.S, c.W, line_start + 1, line_index - 1);
-          const int64_t string_start = string_end - key_len;
+          const Pos string_end = prev_bit(sc, c.S, c.W, Pos(line_start + 1), Pos(line_index - 1));
+          const Pos string_start = string_end - key_len;
           bool mismatch = string_start < line_start || at(c, string_start) != '"';
           for (int i = 0; !mismatch && i < key_len; ++i) {
-            if (ir_at(c, key_pos + i) != at(c, string_start + i + 1)) mismatch = true;
+            if (ir_at(c, key_pos + i) != at(c, Pos(string_start + i + 1))) mismatch = true;
           }
           if (mismatch) {
             ++line_index;
-            line_index = next_struct(c, lbc, level_end[level], line_index, level);
+            line_index = next_struct(c, lbc, lend, line_index, level);
             if (at(c, line_index) == '}') return;
             continue;
           }
@@ -234,33 +255,41 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       }
       ++line_index;
       break;
+    }
     case OP_MOVE_TO_INDEX: {
       target = read_varint(c, qp);
       if (!LEVEL_OK(level)) return;
       const uint8_t ch = at(c, line_index);
       if (ch != '[' && ch != ',' && ch != ']') return;
-      if (ch == '[') curr_index[level] = 0;
-      else ++curr_index[level];
+      int32_t ci = ch == '[' ? 0 : L.curr_index(level) + 1;
+      const Pos lend = L.level_end(level);
       steps = 0;
+      bool fail = false;
       for (;;) {
-        if (++steps > max_steps) return;
-        if (curr_index[level] < target) {
+        if (++steps > max_steps) {
+          fail = true;
+          break;
+        }
+        if (ci < target) {
           ++line_index;
-          line_index = next_struct(c, lbc, level_end[level], line_index, level);
+          line_index = next_struct(c, lbc, lend, line_index, level);
           if (at(c, line_index) == ',') {
-            ++curr_index[level];
+            ++ci;
             continue;
           }
-          return;
+          fail = true;
+          break;
         }
-        if (curr_index[level] > target) {
+        if (ci > target) {
           --line_index;
-          line_index = prev_struct(c, lbc, 0, line_index, level);
-          --curr_index[level];
+          line_index = prev_struct(c, lbc, Pos(0), line_index, level);
+          --ci;
           continue;
         }
         break;
       }
+      L.curr_index(level) = ci;
+      if (fail) return;
       if (at(c, line_index) == ']') return;
       ++line_index;
       break;
@@ -268,32 +297,39 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
     case OP_MOVE_TO_INDEX_REVERSE: {
       target = read_varint(c, qp);
       if (!LEVEL_OK(level)) return;
-      line_index = level_end[level] - 1;
+      line_index = L.level_end(level) - 1;
       while (at(c, line_index) == ' ') --line_index;
       const uint8_t ch = at(c, line_index);
       if (ch != ']' && ch != ',' && ch != '[') return;
-      if (ch == ']') curr_index[level] = 0;
-      else ++curr_index[level];
+      int32_t ci = ch == ']' ? 0 : L.curr_index(level) + 1;
+      const Pos lend = L.level_end(level);
       steps = 0;
+      bool fail = false;
       for (;;) {
-        if (++steps > max_steps) return;
-        if (curr_index[level] < target) {
+        if (++steps > max_steps) {
+          fail = true;
+          break;
+        }
+        if (ci < target) {
           --line_index;
-          line_index = prev_struct(c, lbc, 0, line_index, level);
-          if (at(c, line_index) == ',' || curr_index[level] + 1 == target) {
-            ++curr_index[level];
+          line_index = prev_struct(c, lbc, Pos(0), line_index, level);
+          if (at(c, line_index) == ',' || ci + 1 == target) {
+            ++ci;
             continue;
           }
-          return;
+          fail = true;
+          break;
         }
-        if (curr_index[level] > target) {
+        if (ci > target) {
           ++line_index;
-          line_index = next_struct(c, lbc, level_end[level], line_index, level);
-          --curr_index[level];
+          line_index = next_struct(c, lbc, lend, line_index, level);
+          --ci;
           continue;
         }
         break;
       }
+      L.curr_index(level) = ci;
+      if (fail) return;
       ++line_index;
       break;
     }
@@ -308,10 +344,10 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       line_index = marked_pos[marked];
       level = marked_level[marked];
       --marked;
-      for (int i = level + 1; i < kMaxQueryLevels; ++i) {
+      for (int i = level + 1; i < L.nlev; ++i) {
         if (i < 0) continue;
-        if (level_end[i] == -1) break;
-        level_end[i] = -1;
+        if (L.level_end(i) == -1) break;
+        L.level_end(i) = -1;
       }
       break;
     case OP_EXPRESSION_STRING_EQUALS: {
@@ -319,30 +355,36 @@ __device__ void run_record(const Rec &c, int64_t line_start, int64_t line_end,
       key_pos = qp;
       qp += key_len;
       if (key_len < 0 || !LEVEL_OK(level)) return;
-      while (at(c, line_index) == ' ' && line_index < level_end[level]) ++line_index;
-      int64_t string_end = level_end[level] - 1;
+      const Pos lend = L.level_end(level);
+      while (at(c, line_index) == ' ' && line_index < lend) ++line_index;
+      Pos string_end = lend - 1;
       while (line_index < string_end && at(c, string_end) == ' ') --string_end;
       if (string_end - line_index + 1 != key_len) return;
       for (int i = 0; i < key_len; ++i) {
-        if (ir_at(c, key_pos + i) != at(c, line_index + i)) return;
+        if (ir_at(c, key_pos + i) != at(c, Pos(line_index + i))) return;
       }
       break;
     }
     default:
       break;
     }
-    if (qp > int64_t(c.ir_len) + 1) return;
+    if (qp > c.ir_len + 1) return;
   }
 #undef LEVEL_OK
 }
 
-template <typename OutT>
+template <typename Pos, typename OutT>
 __global__ void __launch_bounds__(256)
-    query_kernel(const QueryLaunch q, const __grid_constant__ IrBlob ir, OutT *out) {
+    query_kernel(const QueryLaunch q, const __grid_constant__ IrBlob ir, OutT *out, int nlev) {
   __shared__ uint8_t s_ir[kMaxQueryIrBytes];
+  extern __shared__ __align__(8) uint8_t s_levels[];  // Pos[nlev][bdim], int32[nlev][bdim]
   for (int i = threadIdx.x; i < q.ir_len; i += blockDim.x) s_ir[i] = ir.bytes[i];
   __syncthreads();
-  const Rec c{q.in, q.n, q.S, q.LB, q.W, s_ir, q.ir_len, q.base_level, q.num_levels};
+  const Rec<Pos> c{q.in, Pos(q.n), q.S, q.LB, Pos(q.W), s_ir, q.ir_len, q.base_level,
+                   q.num_levels};
+  Pos *ends = reinterpret_cast<Pos *>(s_levels);
+  int32_t *idx = reinterpret_cast<int32_t *>(ends + nlev * blockDim.x);
+  const LevelState<Pos> L{ends + threadIdx.x, idx + threadIdx.x, int(blockDim.x), nlev};
   const int64_t stride = int64_t(blockDim.x) * gridDim.x;
   for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < q.num_lines;
        r += stride) {
@@ -350,15 +392,19 @@ __global__ void __launch_bounds__(256)
     for (int i = 0; i < 2 * q.num_results; ++i) o[i] = OutT(-1);
     const int64_t start = q.NL[r];
     const int64_t end = (r + 1 < q.num_lines) ? q.NL[r + 1] : q.n - 1;
-    run_record<OutT>(c, start, end, q.num_results, o);
+    run_record<Pos, OutT>(c, L, Pos(start), Pos(end), q.num_results, o);
   }
 }
 
 __global__ void __launch_bounds__(256)
-    batch_query_kernel(const BatchQueryLaunch q, const __grid_constant__ IrBlob ir) {
+    batch_query_kernel(const BatchQueryLaunch q, const __grid_constant__ IrBlob ir, int nlev) {
   __shared__ uint8_t s_ir[kMaxQueryIrBytes];
+  extern __shared__ __align__(8) uint8_t s_levels[];  // int32[nlev][bdim] x 2
   for (int i = threadIdx.x; i < kMaxQueryIrBytes; i += blockDim.x) s_ir[i] = ir.bytes[i];
   __syncthreads();
+  int32_t *ends = reinterpret_cast<int32_t *>(s_levels);
+  const LevelState<int32_t> L{ends + threadIdx.x, ends + nlev * blockDim.x + threadIdx.x,
+                              int(blockDim.x), nlev};
   const uint64_t records = q.totals[kTotRecords];
   const uint64_t stride = uint64_t(blockDim.x) * gridDim.x;
   for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < records; r += stride) {
@@ -379,17 +425,66 @@ __global__ void __launch_bounds__(256)
     const int64_t *nl = q.NL + row[kFiNlOff];
     const int64_t start = nl[i];
     const int64_t end = (i + 1 < lines) ? nl[i + 1] : int64_t(F.n) - 1;
-    const Rec c{q.in + F.in_off, int64_t(F.n), q.S + F.s_off, q.LB + F.lb_off,
-                int64_t((F.n + 63u) / 64u), s_ir + g.ir_off, g.ir_len, g.base_level, F.levels};
-    run_record<int32_t>(c, start, end, g.num_results, o);
+    // batch files are below 2 GiB (int32 results): 32-bit positions
+    const Rec<int32_t> c{q.in + F.in_off, int32_t(F.n), q.S + F.s_off, q.LB + F.lb_off,
+                         int32_t((F.n + 63u) / 64u), s_ir + g.ir_off, g.ir_len, g.base_level,
+                         F.levels};
+    run_record<int32_t, int32_t>(c, L, int32_t(start), int32_t(end), g.num_results, o);
   }
 }
 
 }  // namespace
 
+int query_ir_levels(const uint8_t *ir, int len) {
+  // Follows the interpreter's level changes along the IR (it has no jumps;
+  // reset returns to a marked level) to find the deepest level it can reach.
+  int level = 0, deepest = 0, marked = 0;
+  int marks[kMaxQueryLevels] = {};
+  auto skip_varint = [&](int &p, int *value) {
+    uint32_t v = 0, b = 0;
+    int shift = 0;
+    while (p < len && ((b = ir[p++]) & 0x80u) != 0 && shift <= 28) {
+      v |= (b & 0x7Fu) << shift;
+      shift += 7;
+    }
+    if (value != nullptr) *value = int(v | (shift <= 28 ? (b << shift) : 0u));
+  };
+  for (int p = 0; p < len;) {
+    const uint8_t op = ir[p++];
+    if (op == OP_END) break;
+    int n = 0;
+    switch (op) {
+    case OP_MOVE_UP: --level; break;
+    case OP_MOVE_DOWN: ++level; break;
+    case OP_MOVE_TO_KEY:
+    case OP_EXPRESSION_STRING_EQUALS:
+      skip_varint(p, &n);
+      if (n > 0) p += n;
+      break;
+    case OP_MOVE_TO_INDEX:
+    case OP_MOVE_TO_INDEX_REVERSE: skip_varint(p, nullptr); break;
+    case OP_MARK_POSITION:
+      if (marked < kMaxQueryLevels) marks[marked++] = level;
+      break;
+    case OP_RESET_POSITION:
+      if (marked > 0) level = marks[--marked];
+      break;
+    default: break;
+    }
+    if (level > deepest) deepest = level;
+  }
+  return deepest + 1 < kMaxQueryLevels ? deepest + 1 : kMaxQueryLevels;
+}
+
 cudaError_t batch_query_launch(const BatchQueryLaunch &q, const IrBlob &ir, int grid,
                                int block, cudaStream_t stream) {
-  batch_query_kernel<<<grid, block, 0, stream>>>(q, ir);
+  int nlev = 1;
+  for (int g = 0; g < q.num_groups; ++g) {
+    const int l = query_ir_levels(ir.bytes + q.groups[g].ir_off, q.groups[g].ir_len);
+    if (l > nlev) nlev = l;
+  }
+  const size_t smem = size_t(nlev) * size_t(block) * 8u;
+  batch_query_kernel<<<grid, block, smem, stream>>>(q, ir, nlev);
   return cudaGetLastError();
 }
 
@@ -399,10 +494,14 @@ cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
   if (block <= 0) block = 256;
   if (block > 256) block = 256;
   if (grid <= 0) grid = int((q.num_lines + block - 1) / block);
+  const int nlev = query_ir_levels(ir.bytes, q.ir_len);
   if (q.out64 != nullptr) {
-    query_kernel<int64_t><<<grid, block, 0, stream>>>(q, ir, q.out64);
+    const size_t smem = size_t(nlev) * size_t(block) * 12u;
+    query_kernel<int64_t, int64_t><<<grid, block, smem, stream>>>(q, ir, q.out64, nlev);
   } else {
-    query_kernel<int32_t><<<grid, block, 0, stream>>>(q, ir, q.out32);
+    // int32 results imply a partition below 2 GiB: 32-bit positions
+    const size_t smem = size_t(nlev) * size_t(block) * 8u;
+    query_kernel<int32_t, int32_t><<<grid, block, smem, stream>>>(q, ir, q.out32, nlev);
   }
   return cudaGetLastError();
 }
