@@ -396,13 +396,30 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
     }
     return;
   }
+  // Every CTA claims about one tile per iteration, so the tiles claimed one
+  // iteration from now are about gridDim.x tiles ahead: that tile's bytes are
+  // prefetched into L2 (its file is looked up beside the current tile's).
+  const uint32_t ahead = t + gridDim.x;
   uint32_t f = 0;
   IndexFile F;
+  uint64_t pf = ~0ull;  // byte offset in P.in of the tile to prefetch
   if (P.files == nullptr) {
     F = P.single;
+    if (ahead < P.num_tiles) pf = uint64_t(ahead) * TILE_BYTES;
   } else {
-    f = P.tile_file ? P.tile_file[t] : file_of_tile(P, t);
+    uint32_t fa = 0;
+    if (P.tile_file) {
+      f = P.tile_file[t];
+      if (ahead < P.num_tiles) fa = P.tile_file[ahead];
+    } else {
+      f = file_of_tile(P, t);
+      if (ahead < P.num_tiles) fa = file_of_tile(P, ahead);
+    }
     F = P.files[f];
+    if (ahead < P.num_tiles) {
+      const IndexFile A = P.files[fa];
+      pf = A.in_off + uint64_t(ahead - A.first_tile) * TILE_BYTES;
+    }
   }
   const uint32_t ktile = t - F.first_tile;
   const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
@@ -430,11 +447,7 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
           " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(sm.tiles[s])),
           "l"(tmap), "r"(0), "r"(int32_t(row0)), "r"(full)
           : "memory");
-      // Every CTA claims about one tile per iteration, so the tiles claimed
-      // one iteration from now lie about gridDim.x tiles ahead: pull that
-      // stretch of the input into L2 so their TMA loads hit it.
-      const uint64_t pf = F.in_off + byte0 + uint64_t(gridDim.x) * TILE_BYTES;
-      if (pf + TILE_BYTES <= P.full_rows * 128u)
+      if (pf != ~0ull && pf + TILE_BYTES <= P.full_rows * 128u)
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.in + pf),
                      "r"(uint32_t(TILE_BYTES))
                      : "memory");
