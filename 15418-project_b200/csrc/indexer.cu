@@ -347,19 +347,14 @@ struct PipeSmem {
   uint32_t abort;
 };
 
-// Shared-memory scratch of the warp-cooperative leveled bitmaps (phase B):
-// per warp, the string-masked open/close/separator words of its 64 words
-// with their entering depths, the list of their open/close events, and the
-// leveled words being assembled (32-bit halves, filled by atomicOr).
-constexpr int kWarpEventCap = 256;
-constexpr int kSharedLevels = 4;  // LMAX up to this uses the shared path
-template <int NT>
+// Shared-memory staging of the leveled bitmaps (phase B): per warp and
+// level, one 64-bit slot for each of the warp's 64 words; a lane only ever
+// touches the slots of its own two words.
+constexpr int kSharedLevels = 8;  // LMAX up to this stages in shared memory
+template <int NT, int LMAX>
 struct LevelScratch {
   static constexpr int NW = NT / 32;
-  uint64_t op[NW][64], cl[NW][64], sp[NW][64];
-  int32_t depth[NW][64];
-  uint16_t events[NW][kWarpEventCap];
-  uint32_t lb[NW][kSharedLevels][128];
+  uint64_t lb[NW][LMAX][64];
 };
 
 // One thread's row between phase A and phase B.
@@ -656,87 +651,63 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
   st.nl_ex = nl_ex;
 }
 
-// Leveled bitmaps of the warp's 64 words (two per lane), with the open/close
-// events spread evenly over the lanes: an event's depth follows from the
-// word's entering depth and two popcounts below it, so every event, and the
-// separator run that follows it, is placed independently of the others.
-// Returns false (nothing written) when the warp has more events than its
-// list holds; the caller then walks them per word.
+// Leveled bitmaps of one lane's two words, walked as one event sequence
+// (word 0, then word 1 with the depth carried over), so a warp iterates as
+// often as its busiest lane has events in both words together.  Separators
+// between two events share one depth; an opening bracket belongs to the
+// level it opens, a closing one to the level it closes (signed-char depth,
+// sharemem/leveled-bitmaps-index.cu:270-300).  Each mask is OR-ed into the
+// lane's own shared-memory slot of its level.
 template <int LMAX, int NT>
-__device__ __forceinline__ bool leveled_warp(LevelScratch<NT> &ls, uint64_t O0, uint64_t C0,
-                                             uint64_t P0, int depth0, uint64_t O1, uint64_t C1,
-                                             uint64_t P1, int depth1, uint64_t (&lb0)[LMAX],
+__device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_t O0,
+                                             uint64_t C0, uint64_t P0, uint64_t O1, uint64_t C1,
+                                             uint64_t P1, int depth0, uint64_t (&lb0)[LMAX],
                                              uint64_t (&lb1)[LMAX]) {
-  static_assert(LMAX <= kSharedLevels, "shared staging holds kSharedLevels levels");
-  const int lane = threadIdx.x & 31, warp = (threadIdx.x >> 5);
-  const uint64_t E0 = O0 | C0, E1 = O1 | C1;
-  const uint32_t cnt = uint32_t(popc64(E0) + popc64(E1));
-  uint32_t inc = cnt;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, off);
-    if (lane >= off) inc += v;
-  }
-  const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
-  if (total > uint32_t(kWarpEventCap)) return false;  // warp-uniform
-  const int w0 = 2 * lane, w1 = 2 * lane + 1;
-  ls.op[warp][w0] = O0;
-  ls.cl[warp][w0] = C0;
-  ls.sp[warp][w0] = P0;
-  ls.depth[warp][w0] = depth0;
-  ls.op[warp][w1] = O1;
-  ls.cl[warp][w1] = C1;
-  ls.sp[warp][w1] = P1;
-  ls.depth[warp][w1] = depth1;
-  // separators before a word's first event sit at its entering depth
-  const uint64_t f0 = E0 & (0 - E0), f1 = E1 & (0 - E1);
-  const uint64_t head0 = P0 & (f0 ? f0 - 1 : ~0ull), head1 = P1 & (f1 ? f1 - 1 : ~0ull);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t *slot = &ls.lb[warp][0][2 * lane];  // [level * 64 + word]
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
-    const uint64_t a = depth0 == l ? head0 : 0ull, b = depth1 == l ? head1 : 0ull;
-    ls.lb[warp][l][2 * w0] = uint32_t(a);
-    ls.lb[warp][l][2 * w0 + 1] = uint32_t(a >> 32);
-    ls.lb[warp][l][2 * w1] = uint32_t(b);
-    ls.lb[warp][l][2 * w1 + 1] = uint32_t(b >> 32);
+    slot[l * 64] = 0ull;
+    slot[l * 64 + 1] = 0ull;
   }
-  uint32_t slot = inc - cnt;
-  for (uint64_t m = E0; m; m &= m - 1) ls.events[warp][slot++] = uint16_t((w0 << 6) | (__ffsll(m) - 1));
-  for (uint64_t m = E1; m; m &= m - 1) ls.events[warp][slot++] = uint16_t((w1 << 6) | (__ffsll(m) - 1));
-  __syncwarp();
-  for (uint32_t i = uint32_t(lane); i < total; i += 32u) {
-    const uint32_t e = ls.events[warp][i];
-    const int w = int(e >> 6), p = int(e & 63u);
-    const uint64_t O = ls.op[warp][w], C = ls.cl[warp][w], Pm = ls.sp[warp][w];
-    const uint64_t bit = 1ull << p, below = bit - 1, upto_me = below | bit;
-    const int before = ls.depth[warp][w] + popc64(O & below) - popc64(C & below);
+  uint64_t O = O0, Pm = P0, ev = O0 | C0, acc = 0, done = 0;
+  int h = 0, d = depth0;
+  for (;;) {
+    if (ev == 0) {
+      // separators after the word's last event
+      const uint64_t m = acc | (Pm & ~done);
+      if (m != 0 && d >= 0 && d < LMAX) slot[d * 64 + h] |= m;
+      if (h == 1) break;
+      h = 1;
+      O = O1;
+      Pm = P1;
+      ev = O1 | C1;
+      acc = 0;
+      done = 0;
+      continue;
+    }
+    const uint64_t bit = ev & (0 - ev);
+    const uint64_t below = bit - 1;
+    acc |= Pm & below & ~done;
     const bool open = (O & bit) != 0;
-    const int lev = int(int8_t(uint8_t(before + (open ? 1 : 0))));     // the event's own level
-    const int after = int(int8_t(uint8_t(before + (open ? 1 : -1))));  // depth after it
-    const uint64_t rest = (O | C) & ~upto_me;
-    const uint64_t nxt = rest & (0 - rest);
-    const uint64_t seg = Pm & ~upto_me & (nxt ? nxt - 1 : ~0ull);
-    if (lev >= 0 && lev < LMAX) {
-      if (p < 32) atomicOr(&ls.lb[warp][lev][2 * w], uint32_t(bit));
-      else atomicOr(&ls.lb[warp][lev][2 * w + 1], uint32_t(bit >> 32));
-    }
-    if (seg != 0 && after >= 0 && after < LMAX) {
-      if (uint32_t(seg)) atomicOr(&ls.lb[warp][after][2 * w], uint32_t(seg));
-      if (uint32_t(seg >> 32)) atomicOr(&ls.lb[warp][after][2 * w + 1], uint32_t(seg >> 32));
-    }
+    const uint64_t m = open ? acc : (acc | bit);
+    if (m != 0 && d >= 0 && d < LMAX) slot[d * 64 + h] |= m;
+    d = int(int8_t(uint8_t(open ? d + 1 : d - 1)));
+    acc = open ? bit : 0ull;
+    done = below | bit;
+    ev &= ev - 1;
   }
-  __syncwarp();
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
-    lb0[l] = (uint64_t(ls.lb[warp][l][2 * w0 + 1]) << 32) | ls.lb[warp][l][2 * w0];
-    lb1[l] = (uint64_t(ls.lb[warp][l][2 * w1 + 1]) << 32) | ls.lb[warp][l][2 * w1];
+    lb0[l] = slot[l * 64];
+    lb1[l] = slot[l * 64 + 1];
   }
-  __syncwarp();  // the scratch is reused by the next tile
-  return true;
 }
 
 template <int LMAX, int NT>
 __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
-                                        LevelScratch<NT> &ls, uint32_t k, const RowState &st) {
+                                        LevelScratch<NT, LMAX> &ls, uint32_t k,
+                                        const RowState &st) {
   constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
   const int tid = threadIdx.x;
   const int j = int(k & 1u);
@@ -766,13 +737,9 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
     uint64_t lb0[LMAX], lb1[LMAX];
     const uint64_t O0 = st.op0 & ~S0, C0 = st.cl0 & ~S0, P0 = st.sp0 & ~S0;
     const uint64_t O1 = st.op1 & ~S1, C1 = st.cl1 & ~S1, P1 = st.sp1 & ~S1;
-    bool done = false;
     if constexpr (LMAX <= kSharedLevels) {
-      // signed-char depth entering word 1
-      const int depth1 = int(int8_t(uint8_t(depth0 + popc64(O0) - popc64(C0))));
-      done = leveled_warp<LMAX, NT>(ls, O0, C0, P0, depth0, O1, C1, P1, depth1, lb0, lb1);
-    }
-    if (!done) {
+      leveled_lane<LMAX, NT>(ls, O0, C0, P0, O1, C1, P1, depth0, lb0, lb1);
+    } else {
       const int depth1 = leveled_word<LMAX>(O0, C0, P0, depth0, lb0);
       leveled_word<LMAX>(O1, C1, P1, depth1, lb1);
     }
@@ -806,7 +773,8 @@ __global__ void __launch_bounds__(NT + 32, LMAX > 8 ? 1 : (NT <= 128 ? 4 : 2))
   // the 128-byte-swizzled TMA destinations need 1024-byte alignment
   uint8_t *smem_base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   PipeSmem<NT> &sm = *reinterpret_cast<PipeSmem<NT> *>(smem_base);
-  LevelScratch<NT> &ls = *reinterpret_cast<LevelScratch<NT> *>(smem_base + level_scratch_offset<NT>());
+  LevelScratch<NT, LMAX> &ls =
+      *reinterpret_cast<LevelScratch<NT, LMAX> *>(smem_base + level_scratch_offset<NT>());
   const int tid = threadIdx.x;
   if (tid == NT) {
     // barriers must be initialised before anyone polls them: shared memory
@@ -856,7 +824,7 @@ template <int LMAX, bool kTma, int NT>
 cudaError_t launch_kernel(const IndexLaunch &L, const CUtensorMap &map, cudaStream_t stream) {
   auto kernel = index_kernel<LMAX, kTma, NT>;
   constexpr size_t smem = level_scratch_offset<NT>() +
-                          (LMAX <= kSharedLevels ? sizeof(LevelScratch<NT>) : 0) +
+                          (LMAX <= kSharedLevels ? sizeof(LevelScratch<NT, LMAX>) : 0) +
                           1024;  // + alignment slack
   static int grid_per_device[64] = {};
   int dev = 0;
