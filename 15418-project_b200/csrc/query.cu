@@ -235,19 +235,24 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       steps = 0;
       for (;;) {
         if (++steps > max_steps) return;
-        ++line_index;
-        line_index = next_struct(c, lbc, lend, line_index, level);
-        if (at(c, line_index) == ':') {
-          const Pos string_end = prev_bit(sc, c.S, c.W, Pos(line_start + 1), Pos(line_index - 1));
-          const Pos string_start = string_end - key_len;
-          bool mismatch = string_start < line_start || at(c, string_start) != '"';
+        // Every position this step may inspect follows from the bitmaps
+        // alone: the next structural character, the key string that would
+        // end before it, and the structural character after it.  Their
+        // bytes are then loaded together rather than one after another.
+        const Pos p1 = next_struct(c, lbc, lend, Pos(line_index + 1), level);
+        const Pos p2 = next_struct(c, lbc, lend, Pos(p1 + 1), level);
+        const Pos string_end = prev_bit(sc, c.S, c.W, Pos(line_start + 1), Pos(p1 - 1));
+        const Pos string_start = string_end - key_len;
+        const uint8_t b1 = at(c, p1), b2 = at(c, p2), bq = at(c, string_start);
+        line_index = p1;
+        if (b1 == ':') {
+          bool mismatch = string_start < line_start || bq != '"';
           for (int i = 0; !mismatch && i < key_len; ++i) {
             if (ir_at(c, key_pos + i) != at(c, Pos(string_start + i + 1))) mismatch = true;
           }
           if (mismatch) {
-            ++line_index;
-            line_index = next_struct(c, lbc, lend, line_index, level);
-            if (at(c, line_index) == '}') return;
+            line_index = p2;
+            if (b2 == '}') return;
             continue;
           }
         }
