@@ -125,10 +125,19 @@ C3_DESC = ("c3: 10,000 seeded files, log-normal sizes 4 KiB-64 MiB, half NDJSON 
 C3_QUERIES = ["$.user.lang", "$[*].categoryPath[1:3].id"]
 
 
-def c3_files(pkg, scale: float = 1.0, limit_bytes: int | None = None):
+def c3_shard_seeds(rank: int) -> tuple[int, int]:
+    """Seeds of one rank's shard of config 3: (size-distribution seed, base
+    seed of its file contents).  Rank 0 is the single-GPU workload; every
+    other rank gets its own 10,000 files (multi-GPU runs shard distinct files
+    over the ranks, weak scaling)."""
+    return 3 + 1000 * rank, 10_000_000 * rank
+
+
+def c3_files(pkg, scale: float = 1.0, limit_bytes: int | None = None, rank: int = 0):
     """10,000 seeded files (even: NDJSON post records, odd: product arrays);
     with limit_bytes only the leading files up to that many bytes."""
-    sizes = c3_sizes(total=int((8 << 30) * scale)) if scale != 1.0 else c3_sizes()
+    size_seed, base = c3_shard_seeds(rank)
+    sizes = c3_sizes(seed=size_seed, total=int((8 << 30) * scale))
     if limit_bytes is not None:
         keep = int(np.searchsorted(np.cumsum(sizes), limit_bytes)) + 1
         sizes = sizes[:keep]
@@ -137,8 +146,8 @@ def c3_files(pkg, scale: float = 1.0, limit_bytes: int | None = None):
     def make(i):
         n = int(sizes[i])
         if i % 2 == 0:
-            return bytes(dg.tweets(3_000_000 + i, n)), 0
-        return bytes(dg.products(4_000_000 + i, n)), 1
+            return bytes(dg.tweets(base + 3_000_000 + i, n)), 0
+        return bytes(dg.products(base + 4_000_000 + i, n)), 1
 
     with cf.ThreadPoolExecutor(os.cpu_count() or 4) as pool:
         return list(pool.map(make, range(len(sizes))))
@@ -376,6 +385,17 @@ def allreduce_max(x: float, world: int) -> float:
     return float(t.item())
 
 
+def allreduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(world: int):
     if world > 1:
         import torch.distributed as dist
@@ -522,7 +542,7 @@ def run_batch(args, world, rank, local):
     import torch
     pkg = entry.package()
     pkg.load_library()
-    files = c3_files(pkg, args.scale)
+    files = c3_files(pkg, args.scale, rank=rank)
     comp = compile_all(pkg, C3_QUERIES)
     queries = [(c, base, c.max_depth + base) for c, base in comp]
     buf, offsets = pkg.pack_files([d for d, _ in files])
@@ -594,7 +614,7 @@ def run_batch(args, world, rank, local):
     assert torch.equal(h_out[: int(v.result_ints)], want)
     e2e_ms = allreduce_max(float(np.mean(e2e)), world)
 
-    gb = total * world / 1e9
+    gb = allreduce_sum(float(total), world) / 1e9  # every rank indexes its own files
     peak, peak_kind = measured_peak_hbm()
     achieved = b_index / (ms_index / 1e3) / 1e9
     chain = (b_index + b_query) / (ms_step / 1e3) / 1e9
@@ -611,7 +631,7 @@ def run_batch(args, world, rank, local):
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
         "config": {"workload": C3_DESC, "input_bytes": total, "files": len(files), "records": int(v.num_records),
-                   "l2": "input larger than L2", "parallelism": f"replicas x{world}",
+                   "l2": "input larger than L2", "parallelism": f"file shards x{world}",
                    "launch_shape": {"index_threads": v.index_threads,
                                     "query_block": v.query_block, "query_grid": v.query_grid,
                                     "graph": bool(v.uses_graph)}},
