@@ -45,7 +45,8 @@ def to_device(data: np.ndarray, offset: int = 0) -> tuple[torch.Tensor, int]:
     """Copies bytes to a fresh device buffer at `offset`; returns (tensor, ptr)."""
     t = torch.zeros(data.size + offset + 256, dtype=torch.uint8, device="cuda")
     if data.size:
-        t[offset:offset + data.size] = torch.from_numpy(np.ascontiguousarray(data))
+        src = data if data.flags.writeable else data.copy()
+        t[offset:offset + data.size] = torch.from_numpy(np.ascontiguousarray(src))
     return t, t.data_ptr() + offset
 
 
