@@ -532,8 +532,55 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(data, comp, records, levels, budget_s=12.0)
+    if rank == 0 and args.ref_gpu:
+        line["reference_gpu"] = reference_gpu(data, queries, records, levels, ms_index,
+                                              ms_step - ms_index)
     ctx.close()
     return line
+
+
+REF_DUMP = ROOT / "oracle" / "_ref" / "ref_dump"
+
+
+def reference_gpu(data, queries, records, levels, ours_index_ms, ours_query_ms):
+    """The reference's own index builders and query executor (its library
+    compiled from its own sources into oracle/_ref) timed on the same GPU and
+    input with CUDA events.  Array-record workloads: the reference indexes the
+    array file and runs the queries on its NDJSON normalisation (it has no
+    "$[*]").  Not a bench value of this engine: a comparison column."""
+    import tempfile
+    if not REF_DUMP.exists():
+        return {"unavailable": "oracle/_ref/ref_dump not built"}
+    out = {"source": "reference library built from its own sources (oracle/ref/build_ref.py)",
+           "ours_index_ms": round(ours_index_ms, 4), "ours_query_ms": round(ours_query_ms, 4)}
+    with tempfile.TemporaryDirectory() as d:
+        raw = Path(d) / "input.json"
+        np.asarray(data).tofile(raw)
+        qfile, qtext = raw, list(queries)
+        if records == "array":
+            b = bytes(np.asarray(data))
+            elems = [ln.rstrip(b",") for ln in b.split(b"\n") if ln not in (b"[", b"]", b"")]
+            qfile = Path(d) / "records.ndjson"
+            qfile.write_bytes(b"\n".join(elems) + b"\n")
+            qtext = ["$" + q[4:] if q.startswith("$[*]") else q for q in queries]
+        for name, builder in (("SHAREMEM", 3), ("COMBINED", 1)):
+            env = dict(os.environ, REF_TIME_REPS="5")
+            r = subprocess.run([str(REF_DUMP), str(raw), str(builder), str(levels),
+                                str(Path(d) / name)], capture_output=True, text=True, env=env,
+                               timeout=900)
+            q = subprocess.run([str(REF_DUMP), str(qfile), str(builder), str(levels),
+                                str(Path(d) / (name + "_q"))] + qtext,
+                               capture_output=True, text=True, env=env, timeout=900)
+            import re
+            mi = re.search(r"ms_index ([0-9.]+) ms_query ([0-9.]+)", r.stdout)
+            mq = re.search(r"ms_index ([0-9.]+) ms_query ([0-9.]+)", q.stdout)
+            if r.returncode != 0 or q.returncode != 0 or mi is None or mq is None:
+                out[name] = {"error": (r.stderr + q.stderr + r.stdout[-200:])[-400:]}
+                continue
+            ms_i, ms_q = float(mi.group(1)), float(mq.group(2))
+            out[name] = {"index_ms": round(ms_i, 3), "query_ms": round(ms_q, 3),
+                         "index_speedup_ours": round(ms_i / ours_index_ms, 2)}
+    return out
 
 
 def run_batch(args, world, rank, local):
@@ -779,6 +826,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="c3 only: fraction of the 8 GiB total (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="c0-c2: also time the reference's own library on the same GPU")
     ap.add_argument("--size-mib", type=int, default=None,
                     help="profiling: run the workload's generator at this size")
     args = ap.parse_args()
