@@ -107,14 +107,19 @@ __device__ Pos prev_bit(WordCache<Pos> &wc, const uint64_t *bm, Pos W, Pos min_i
   return -1;
 }
 
+// Leveled-bitmap words of a query level, or null for a level the index does
+// not hold (it has no structural characters).
+template <typename Pos>
+__device__ __forceinline__ const uint64_t *level_words(const Rec<Pos> &c, int level) {
+  const int l = level + c.base;
+  return (l < 0 || l >= c.levels) ? nullptr : c.LB + uint64_t(c.W) * uint64_t(l);
+}
+
 // query.cu:79-115
 template <typename Pos>
 __device__ Pos next_struct(const Rec<Pos> &c, WordCache<Pos> &wc, Pos level_end, Pos line_index,
-                           int level) {
-  if (line_index >= level_end) return level_end;
-  // a level the index does not hold has no structural characters
-  if (level + c.base < 0 || level + c.base >= c.levels) return level_end;
-  const uint64_t *lvl = c.LB + uint64_t(c.W) * uint64_t(level + c.base);
+                           const uint64_t *lvl) {
+  if (line_index >= level_end || lvl == nullptr) return level_end;
   Pos wi = line_index >> 6;
   Pos base = wi * 64;
   uint64_t word = cached_word(wc, lvl, c.W, wi) & (~0ull << (line_index - base));
@@ -134,10 +139,8 @@ __device__ Pos next_struct(const Rec<Pos> &c, WordCache<Pos> &wc, Pos level_end,
 // query.cu:117-128
 template <typename Pos>
 __device__ Pos prev_struct(const Rec<Pos> &c, WordCache<Pos> &wc, Pos level_start, Pos line_index,
-                           int level) {
-  if (line_index <= level_start) return level_start;
-  if (level + c.base < 0 || level + c.base >= c.levels) return level_start;
-  const uint64_t *lvl = c.LB + uint64_t(c.W) * uint64_t(level + c.base);
+                           const uint64_t *lvl) {
+  if (line_index <= level_start || lvl == nullptr) return level_start;
   const Pos s = prev_bit(wc, lvl, c.W, level_start, line_index);
   return s == -1 ? level_start : s;
 }
@@ -221,7 +224,8 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       if (!LEVEL_OK(level) || level < 1) return;
       if (L.level_end(level) == -1) {
         L.level_end(level) =
-            next_struct(c, lbc, L.level_end(level - 1), Pos(line_index + 1), level - 1);
+            next_struct(c, lbc, L.level_end(level - 1), Pos(line_index + 1),
+                        level_words(c, level - 1));
         while (at(c, line_index) == ' ') ++line_index;
       }
       break;
@@ -232,6 +236,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       if (key_len < 0 || !LEVEL_OK(level)) return;
       if (at(c, line_index) != '{') return;
       const Pos lend = L.level_end(level);
+      const uint64_t *lvl = level_words(c, level);
       steps = 0;
       for (;;) {
         if (++steps > max_steps) return;
@@ -239,8 +244,8 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
         // alone: the next structural character, the key string that would
         // end before it, and the structural character after it.  Their
         // bytes are then loaded together rather than one after another.
-        const Pos p1 = next_struct(c, lbc, lend, Pos(line_index + 1), level);
-        const Pos p2 = next_struct(c, lbc, lend, Pos(p1 + 1), level);
+        const Pos p1 = next_struct(c, lbc, lend, Pos(line_index + 1), lvl);
+        const Pos p2 = next_struct(c, lbc, lend, Pos(p1 + 1), lvl);
         const Pos string_end = prev_bit(sc, c.S, c.W, Pos(line_start + 1), Pos(p1 - 1));
         const Pos string_start = string_end - key_len;
         const uint8_t b1 = at(c, p1), b2 = at(c, p2), bq = at(c, string_start);
@@ -268,6 +273,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       if (ch != '[' && ch != ',' && ch != ']') return;
       int32_t ci = ch == '[' ? 0 : L.curr_index(level) + 1;
       const Pos lend = L.level_end(level);
+      const uint64_t *lvl = level_words(c, level);
       steps = 0;
       bool fail = false;
       for (;;) {
@@ -277,7 +283,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
         }
         if (ci < target) {
           ++line_index;
-          line_index = next_struct(c, lbc, lend, line_index, level);
+          line_index = next_struct(c, lbc, lend, line_index, lvl);
           if (at(c, line_index) == ',') {
             ++ci;
             continue;
@@ -287,7 +293,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
         }
         if (ci > target) {
           --line_index;
-          line_index = prev_struct(c, lbc, Pos(0), line_index, level);
+          line_index = prev_struct(c, lbc, Pos(0), line_index, lvl);
           --ci;
           continue;
         }
@@ -308,6 +314,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       if (ch != ']' && ch != ',' && ch != '[') return;
       int32_t ci = ch == ']' ? 0 : L.curr_index(level) + 1;
       const Pos lend = L.level_end(level);
+      const uint64_t *lvl = level_words(c, level);
       steps = 0;
       bool fail = false;
       for (;;) {
@@ -317,7 +324,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
         }
         if (ci < target) {
           --line_index;
-          line_index = prev_struct(c, lbc, Pos(0), line_index, level);
+          line_index = prev_struct(c, lbc, Pos(0), line_index, lvl);
           if (at(c, line_index) == ',' || ci + 1 == target) {
             ++ci;
             continue;
@@ -327,7 +334,7 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
         }
         if (ci > target) {
           ++line_index;
-          line_index = next_struct(c, lbc, lend, line_index, level);
+          line_index = next_struct(c, lbc, lend, line_index, lvl);
           --ci;
           continue;
         }
