@@ -388,6 +388,7 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
     if (lane == 0) {
       sm.stage[s].tile = kEndTile;
       mbar_arrive(full);
+      mbar_arrive(full);
     }
     return;
   }
@@ -418,20 +419,12 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
   }
   const uint32_t ktile = t - F.first_tile;
   const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
-  // escape carry: parity of the backslash run ending the word before the
-  // tile, counted inside that word (all 64 bytes read at once)
-  uint32_t halo = 0;
-  if (ktile != 0) {
-    const uint8_t *w = P.in + F.in_off + byte0 - 64u;
-    const uint32_t lo = __ballot_sync(0xFFFFFFFFu, w[lane] != '\\');
-    const uint32_t hi = __ballot_sync(0xFFFFFFFFu, w[32 + lane] != '\\');
-    const uint64_t not_bs = (uint64_t(hi) << 32) | lo;
-    halo = uint32_t(__clzll(static_cast<long long>(not_bs))) & 1u;
-  }
+  // The stage's barrier takes two arrivals: one with the copy's byte count
+  // as soon as the copy is issued, one once the escape carry (a dependent
+  // global load) is written, so the copy does not wait for that load.
   if (lane == 0) {
     sm.stage[s].tile = t;
     sm.stage[s].file_idx = f;
-    sm.stage[s].halo = halo;
     sm.stage[s].F = F;
     if constexpr (kTma) {
       const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
@@ -449,6 +442,20 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
     } else {
       mbar_arrive(full);
     }
+  }
+  // escape carry: parity of the backslash run ending the word before the
+  // tile, counted inside that word (all 64 bytes read at once)
+  uint32_t halo = 0;
+  if (ktile != 0) {
+    const uint8_t *w = P.in + F.in_off + byte0 - 64u;
+    const uint32_t lo = __ballot_sync(0xFFFFFFFFu, w[lane] != '\\');
+    const uint32_t hi = __ballot_sync(0xFFFFFFFFu, w[32 + lane] != '\\');
+    const uint64_t not_bs = (uint64_t(hi) << 32) | lo;
+    halo = uint32_t(__clzll(static_cast<long long>(not_bs))) & 1u;
+  }
+  if (lane == 0) {
+    sm.stage[s].halo = halo;
+    mbar_arrive(full);
   }
   tile_out = t;
 }
@@ -781,7 +788,7 @@ __global__ void __launch_bounds__(NT + 32, LMAX > 8 ? 1 : (NT <= 128 ? 4 : 2))
     // may still hold barriers of an earlier CTA on this SM
 #pragma unroll
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(smem_u32(&sm.full[s]), 1);
+      mbar_init(smem_u32(&sm.full[s]), 2);  // copy issued + escape carry written
       sm.stage[s].tile = kEndTile;
     }
 #pragma unroll
