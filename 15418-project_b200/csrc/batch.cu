@@ -37,6 +37,7 @@ struct gpj_batch {
   // device state
   gpjb::IndexFile *d_files = nullptr;
   uint32_t *d_tile_file = nullptr;
+  uint32_t *d_tile_row = nullptr;
   std::vector<uint64_t> host_lines;  // per-file line counts (sizing pass)
   std::vector<uint64_t> host_info;   // file info rows of the sizing pass
   uint32_t *d_query_of_file = nullptr;
@@ -98,6 +99,7 @@ int bind_launch(gpj_batch *b) {
   L.full_rows = b->input_bytes / 128u;
   L.files = b->d_files;
   L.tile_file = b->d_tile_file;
+  L.tile_row = b->d_tile_row;
   L.num_files = b->num_files;
   L.num_levels = b->max_levels;
   L.S = b->d_S;
@@ -146,6 +148,7 @@ void release(gpj_batch *b) {
   if (b->stream) cudaStreamDestroy(b->stream);
   cudaFree(b->d_files);
   cudaFree(b->d_tile_file);
+  cudaFree(b->d_tile_row);
   cudaFree(b->d_query_of_file);
   cudaFree(b->d_slots);
   cudaFree(b->d_S);
@@ -163,10 +166,12 @@ int alloc_layout_buffers(gpj_batch *b) {
   cudaFree(b->d_scratch);
   cudaFree(b->d_files);
   cudaFree(b->d_tile_file);
+  cudaFree(b->d_tile_row);
   b->d_S = b->d_LB = nullptr;
   b->d_scratch = nullptr;
   b->d_files = nullptr;
   b->d_tile_file = nullptr;
+  b->d_tile_row = nullptr;
   BCUDA(cudaMalloc(&b->d_S, (b->s_words + 2) * 8u), "cudaMalloc S");
   BCUDA(cudaMalloc(&b->d_LB, (b->lb_words + 2) * 8u), "cudaMalloc LB");
   BCUDA(cudaMalloc(&b->d_scratch, (uint64_t(b->L.num_tiles) * 8u + 64u + 255u) & ~uint64_t(255)),
@@ -175,15 +180,30 @@ int alloc_layout_buffers(gpj_batch *b) {
   BCUDA(cudaMemcpy(b->d_files, b->files.data(), b->files.size() * sizeof(gpjb::IndexFile),
                    cudaMemcpyHostToDevice),
         "copy file table");
-  std::vector<uint32_t> tile_file(b->L.num_tiles);
+  // per tile: its file, and its first 128-byte input row (bit 31: the file's
+  // first tile), so the indexer can start a tile's copy after one load
+  std::vector<uint32_t> tile_file(b->L.num_tiles), tile_row(b->L.num_tiles);
   for (uint32_t f = 0; f < b->num_files; ++f) {
     const uint32_t end = (f + 1 < b->num_files) ? b->files[f + 1].first_tile : b->L.num_tiles;
-    for (uint32_t t = b->files[f].first_tile; t < end; ++t) tile_file[t] = f;
+    const uint64_t row = b->files[f].in_off / 128u;
+    for (uint32_t t = b->files[f].first_tile; t < end; ++t) {
+      tile_file[t] = f;
+      tile_row[t] = uint32_t(row + uint64_t(t - b->files[f].first_tile) * b->index_threads) |
+                    (t == b->files[f].first_tile ? 0x80000000u : 0u);
+    }
   }
   BCUDA(cudaMalloc(&b->d_tile_file, (tile_file.size() + 1) * 4u), "cudaMalloc tile map");
   BCUDA(cudaMemcpy(b->d_tile_file, tile_file.data(), tile_file.size() * 4u,
                    cudaMemcpyHostToDevice),
         "copy tile map");
+  // row numbers take 31 bits (inputs below 256 GiB); beyond that the
+  // indexer finds a tile's row through the file table
+  if (b->input_bytes / 128u + uint64_t(b->index_threads) < 0x80000000ull) {
+    BCUDA(cudaMalloc(&b->d_tile_row, (tile_row.size() + 1) * 4u), "cudaMalloc tile rows");
+    BCUDA(cudaMemcpy(b->d_tile_row, tile_row.data(), tile_row.size() * 4u,
+                     cudaMemcpyHostToDevice),
+          "copy tile rows");
+  }
   return bind_launch(b);
 }
 

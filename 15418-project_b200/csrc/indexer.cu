@@ -394,40 +394,51 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
   }
   // Every CTA claims about one tile per iteration, so the tiles claimed one
   // iteration from now are about gridDim.x tiles ahead: that tile's bytes are
-  // prefetched into L2 (its file is looked up beside the current tile's).
+  // prefetched into L2.  The copy needs only the tile's first input row: one
+  // load from the row table of a file table, none for a single file.
   const uint32_t ahead = t + gridDim.x;
+  const bool has_ahead = ahead < P.num_tiles;
   uint32_t f = 0;
   IndexFile F;
-  uint64_t pf = ~0ull;  // byte offset in P.in of the tile to prefetch
+  uint64_t row0 = 0, pf_row = ~0ull;
+  bool first = false, have_F = true;
   if (P.files == nullptr) {
     F = P.single;
-    if (ahead < P.num_tiles) pf = uint64_t(ahead) * TILE_BYTES;
+    row0 = uint64_t(t) * NT;
+    first = t == 0;
+    if (has_ahead) pf_row = uint64_t(ahead) * NT;
+  } else if (P.tile_row != nullptr && P.tile_file != nullptr) {
+    const uint32_t tr = P.tile_row[t];
+    f = P.tile_file[t];
+    const uint32_t ta = has_ahead ? P.tile_row[ahead] : 0u;
+    row0 = tr & 0x7FFFFFFFu;
+    first = (tr >> 31) != 0;
+    if (has_ahead) pf_row = ta & 0x7FFFFFFFu;
+    have_F = false;  // loaded after the copy is issued
   } else {
     uint32_t fa = 0;
     if (P.tile_file) {
       f = P.tile_file[t];
-      if (ahead < P.num_tiles) fa = P.tile_file[ahead];
+      if (has_ahead) fa = P.tile_file[ahead];
     } else {
       f = file_of_tile(P, t);
-      if (ahead < P.num_tiles) fa = file_of_tile(P, ahead);
+      if (has_ahead) fa = file_of_tile(P, ahead);
     }
     F = P.files[f];
-    if (ahead < P.num_tiles) {
+    const uint32_t ktile = t - F.first_tile;
+    row0 = (F.in_off + uint64_t(ktile) * TILE_BYTES) / 128u;
+    first = ktile == 0;
+    if (has_ahead) {
       const IndexFile A = P.files[fa];
-      pf = A.in_off + uint64_t(ahead - A.first_tile) * TILE_BYTES;
+      pf_row = (A.in_off + uint64_t(ahead - A.first_tile) * TILE_BYTES) / 128u;
     }
   }
-  const uint32_t ktile = t - F.first_tile;
-  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
   // The stage's barrier takes two arrivals: one with the copy's byte count
   // as soon as the copy is issued, one once the escape carry (a dependent
-  // global load) is written, so the copy does not wait for that load.
+  // global load) and the tile's file are written, so the copy waits for
+  // neither.
   if (lane == 0) {
-    sm.stage[s].tile = t;
-    sm.stage[s].file_idx = f;
-    sm.stage[s].F = F;
     if constexpr (kTma) {
-      const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive_tx(full, uint32_t(TILE_BYTES));
       asm volatile(
@@ -435,25 +446,29 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
           " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(sm.tiles[s])),
           "l"(tmap), "r"(0), "r"(int32_t(row0)), "r"(full)
           : "memory");
-      if (pf != ~0ull && pf + TILE_BYTES <= P.full_rows * 128u)
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.in + pf),
+      if (pf_row != ~0ull && (pf_row + NT) * 128u <= P.full_rows * 128u)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.in + pf_row * 128u),
                      "r"(uint32_t(TILE_BYTES))
                      : "memory");
     } else {
       mbar_arrive(full);
     }
   }
+  if (!have_F) F = P.files[f];
   // escape carry: parity of the backslash run ending the word before the
   // tile, counted inside that word (all 64 bytes read at once)
   uint32_t halo = 0;
-  if (ktile != 0) {
-    const uint8_t *w = P.in + F.in_off + byte0 - 64u;
+  if (!first) {
+    const uint8_t *w = P.in + row0 * 128u - 64u;
     const uint32_t lo = __ballot_sync(0xFFFFFFFFu, w[lane] != '\\');
     const uint32_t hi = __ballot_sync(0xFFFFFFFFu, w[32 + lane] != '\\');
     const uint64_t not_bs = (uint64_t(hi) << 32) | lo;
     halo = uint32_t(__clzll(static_cast<long long>(not_bs))) & 1u;
   }
   if (lane == 0) {
+    sm.stage[s].tile = t;
+    sm.stage[s].file_idx = f;
+    sm.stage[s].F = F;
     sm.stage[s].halo = halo;
     mbar_arrive(full);
   }

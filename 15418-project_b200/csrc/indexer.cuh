@@ -35,6 +35,8 @@ struct IndexLaunch {
   IndexFile single;             // the file when `files` is null (one partition)
   const IndexFile *files = nullptr;  // device table, num_files entries, or null
   const uint32_t *tile_file = nullptr;  // file of each tile (optional; else binary search)
+  const uint32_t *tile_row = nullptr;   // with tile_file: first 128-byte input row of each
+                                        // tile, bit 31 set on a file's first tile (optional)
   uint32_t num_files = 1;
   int num_levels = 0;           // max L over the files (selects the kernel)
   uint64_t *S = nullptr;        // string mask words
