@@ -68,13 +68,17 @@ __device__ Agg lookback(const IndexLaunch &P, uint32_t tile) {
   for (;;) {
     // lane l covers tiles base - 4l - j, j = 0 (newest) .. 3 (oldest)
     uint64_t s[kLookbackPerLane];
+#pragma unroll
+    for (int j = 0; j < kLookbackPerLane; ++j) s[j] = 0;  // not yet published
     uint32_t polls = 0;
     for (;;) {
+      // only descriptors not yet published are (re)read: the lines of the
+      // newest tiles are the ones every look-back polls
       bool ready = true;
 #pragma unroll
       for (int j = 0; j < kLookbackPerLane; ++j) {
         const int64_t idx = base - int64_t(kLookbackPerLane) * lane - j;
-        s[j] = (idx >= 0) ? ld_relaxed(&P.tile_state[idx]) : kStatusIncl;
+        if ((s[j] & 3u) == 0) s[j] = (idx >= 0) ? ld_relaxed(&P.tile_state[idx]) : kStatusIncl;
         ready = ready && ((s[j] & 3u) != 0);
       }
       if (__all_sync(0xFFFFFFFFu, ready)) break;
@@ -85,7 +89,7 @@ __device__ Agg lookback(const IndexLaunch &P, uint32_t tile) {
           if ((s[j] & 3u) == 0) s[j] = kStatusIncl;
         break;
       }
-      __nanosleep(polls < 64 ? 20 : 500);
+      __nanosleep(polls < 4096 ? 32 : 500);
     }
     // fold the lane's descriptors newest-first, stopping at an inclusive one
     uint64_t v = 0;
