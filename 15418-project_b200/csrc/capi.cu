@@ -25,6 +25,9 @@ struct gpj_ctx {
   void *host_results = nullptr;
   uint64_t host_results_bytes = 0;
   unsigned long long *pinned = nullptr;  // 8 words of pinned host memory
+  // host inputs arrive in pieces on a copy stream (created on first use)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t piece_ready = nullptr;
 };
 
 namespace {
@@ -121,6 +124,66 @@ int enqueue_index(gpj_ctx *ctx, const uint8_t *in, uint64_t n, int levels,
     return GPJ_OK;
   }
   GPJ_CUDA(gpjb::index_launch(L, tma ? &map : nullptr, tma, stream), "index kernel launch");
+  return GPJ_OK;
+}
+
+// Pieces of a host input: copied in this many tiles at a time on the copy
+// stream, each piece indexed as soon as it has arrived, so the index of one
+// piece overlaps the copy of the next.
+constexpr uint32_t kIngestPieceTiles = 1024;  // 32 MiB
+
+// Copies n host bytes to d_in (256-byte aligned) and indexes them on
+// `stream`: inputs of more than one piece are copied piece by piece on the
+// context's copy stream, and one indexer launch per piece claims its tiles
+// once the piece is on the device (the look-back reads the finished
+// descriptors of the pieces before it).
+int enqueue_index_from_host(gpj_ctx *ctx, const uint8_t *h_in, uint8_t *d_in, uint64_t n,
+                            int levels, const gpj_index &out, cudaStream_t stream) {
+  const uint64_t piece = uint64_t(kIngestPieceTiles) * gpjb::kTileBytes;
+  if (n <= piece) {
+    if (n > 0)
+      GPJ_CUDA(cudaMemcpyAsync(d_in, h_in, n, cudaMemcpyHostToDevice, stream), "copy input");
+    return enqueue_index(ctx, d_in, n, levels, 0u, out, stream);
+  }
+  if (ctx->copy_stream == nullptr)
+    GPJ_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking),
+             "cudaStreamCreate");
+  if (ctx->piece_ready == nullptr)
+    GPJ_CUDA(cudaEventCreateWithFlags(&ctx->piece_ready, cudaEventDisableTiming),
+             "cudaEventCreate");
+  gpjb::IndexLaunch L;
+  L.in = d_in;
+  L.single.n = n;
+  L.single.levels = levels;
+  L.num_levels = levels;
+  L.full_rows = n / 128u;
+  L.S = out.d_string;
+  L.LB = out.d_leveled;
+  L.NL = out.d_newline;
+  L.nl_cap = out.newline_capacity;
+  L.num_tiles = uint32_t(gpjb::index_num_tiles(n));
+  int rc = ensure(ctx->scratch, ctx->scratch_bytes, gpjb::index_scratch_bytes(n));
+  if (rc != GPJ_OK) return rc;
+  gpjb::index_bind_scratch(L, ctx->scratch);
+  CUtensorMap map;
+  const bool tma = gpjb::index_make_tensor_map(&map, d_in, n);
+  GPJ_CUDA(gpjb::index_clear_scratch(L, stream), "cudaMemsetAsync");
+  // the copies start after the work already queued on `stream`
+  GPJ_CUDA(cudaEventRecord(ctx->piece_ready, stream), "cudaEventRecord");
+  GPJ_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->piece_ready, 0), "cudaStreamWaitEvent");
+  for (uint32_t t0 = 0; t0 < L.num_tiles; t0 += kIngestPieceTiles) {
+    const uint32_t t1 = t0 + kIngestPieceTiles < L.num_tiles ? t0 + kIngestPieceTiles : L.num_tiles;
+    const uint64_t b0 = uint64_t(t0) * gpjb::kTileBytes;
+    const uint64_t b1 = uint64_t(t1) * gpjb::kTileBytes < n ? uint64_t(t1) * gpjb::kTileBytes : n;
+    GPJ_CUDA(cudaMemcpyAsync(d_in + b0, h_in + b0, b1 - b0, cudaMemcpyHostToDevice,
+                             ctx->copy_stream),
+             "copy input piece");
+    GPJ_CUDA(cudaEventRecord(ctx->piece_ready, ctx->copy_stream), "cudaEventRecord");
+    GPJ_CUDA(cudaStreamWaitEvent(stream, ctx->piece_ready, 0), "cudaStreamWaitEvent");
+    GPJ_CUDA(gpjb::index_clear_counter(L, stream), "cudaMemsetAsync");
+    GPJ_CUDA(gpjb::index_launch_range(L, tma ? &map : nullptr, tma, stream, t0, t1),
+             "index kernel launch");
+  }
   return GPJ_OK;
 }
 
@@ -280,6 +343,8 @@ int gpj_ctx_destroy(gpj_ctx *ctx) {
   cudaFree(ctx->host_index);
   cudaFree(ctx->host_results);
   cudaFreeHost(ctx->pinned);
+  if (ctx->piece_ready) cudaEventDestroy(ctx->piece_ready);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   delete ctx;
   return GPJ_OK;
 }
@@ -441,9 +506,7 @@ int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes, in
     ix.newline_capacity = cap;
     ix.num_words = W;
     ix.num_levels = num_levels;
-    if (n > 0)
-      GPJ_CUDA(cudaMemcpyAsync(d_in, h_input, n, cudaMemcpyHostToDevice, stream), "copy input");
-    rc = enqueue_index(ctx, d_in, n, num_levels, 0u, ix, stream);
+    rc = enqueue_index_from_host(ctx, h_input, d_in, n, num_levels, ix, stream);
     uint64_t lines = 0;
     int in_string = 0, depth = -1;
     if (rc == GPJ_OK) rc = read_summary(ctx, n, stream, &lines, &in_string, &depth);

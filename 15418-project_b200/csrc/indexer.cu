@@ -383,10 +383,10 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
   constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
   const int lane = threadIdx.x & 31;
   uint32_t t = 0;
-  if (lane == 0) t = atomicAdd(P.tile_counter, 1u);
+  if (lane == 0) t = P.tile_begin + atomicAdd(P.tile_counter, 1u);
   t = __shfl_sync(0xFFFFFFFFu, t, 0);
   const uint32_t full = smem_u32(&sm.full[s]);
-  if (t >= P.num_tiles) {
+  if (t >= P.tile_end) {
     ended = true;
     tile_out = kEndTile;
     if (lane == 0) {
@@ -401,7 +401,7 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
   // prefetched into L2.  The copy needs only the tile's first input row: one
   // load from the row table of a file table, none for a single file.
   const uint32_t ahead = t + gridDim.x;
-  const bool has_ahead = ahead < P.num_tiles;
+  const bool has_ahead = ahead < P.tile_end;
   uint32_t f = 0;
   IndexFile F;
   uint64_t row0 = 0, pf_row = ~0ull;
@@ -868,7 +868,7 @@ cudaError_t launch_kernel(const IndexLaunch &L, const CUtensorMap &map, cudaStre
     if (e != cudaSuccess) return e;
     grid_per_device[dev] = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   }
-  const uint32_t grid = min(L.num_tiles, uint32_t(grid_per_device[dev]));
+  const uint32_t grid = min(L.tile_end - L.tile_begin, uint32_t(grid_per_device[dev]));
   kernel<<<grid, NT + 32, smem, stream>>>(map, L);
   return cudaGetLastError();
 }
@@ -933,14 +933,31 @@ bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n, int 
   return r == CUDA_SUCCESS;
 }
 
+cudaError_t index_clear_scratch(const IndexLaunch &L, cudaStream_t stream) {
+  return cudaMemsetAsync(L.tile_state, 0, uint64_t(L.num_tiles) * 8u + 64u, stream);
+}
+
+cudaError_t index_clear_counter(const IndexLaunch &L, cudaStream_t stream) {
+  return cudaMemsetAsync(L.tile_counter, 0, sizeof(unsigned int), stream);
+}
+
+cudaError_t index_launch_range(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
+                               cudaStream_t stream, uint32_t t0, uint32_t t1, int threads) {
+  if (t1 > L.num_tiles) t1 = L.num_tiles;
+  if (t0 >= t1) return cudaSuccess;
+  IndexLaunch R = L;
+  R.tile_begin = t0;
+  R.tile_end = t1;
+  if (threads == 128) return launch_threads<128>(R, map, use_tma, stream);
+  return launch_threads<256>(R, map, use_tma, stream);
+}
+
 cudaError_t index_launch(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
                          cudaStream_t stream, int threads) {
   if (L.num_tiles == 0) return cudaSuccess;
-  const uint64_t scratch = uint64_t(L.num_tiles) * 8u + 64u;
-  cudaError_t e = cudaMemsetAsync(L.tile_state, 0, scratch, stream);
+  cudaError_t e = index_clear_scratch(L, stream);
   if (e != cudaSuccess) return e;
-  if (threads == 128) return launch_threads<128>(L, map, use_tma, stream);
-  return launch_threads<256>(L, map, use_tma, stream);
+  return index_launch_range(L, map, use_tma, stream, 0u, L.num_tiles, threads);
 }
 }  // namespace gpjb
 

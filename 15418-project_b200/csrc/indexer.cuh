@@ -53,6 +53,8 @@ struct IndexLaunch {
   unsigned int *error = nullptr;
   unsigned long long *summary = nullptr;  // [0] lines [1] in-string [2] depth
   uint32_t num_tiles = 0;
+  // tiles this launch claims: [tile_begin, tile_end); set by the launchers
+  uint32_t tile_begin = 0, tile_end = 0;
 };
 
 // Error bits the kernels raise in IndexLaunch::error.
@@ -90,6 +92,17 @@ bool index_make_tensor_map(CUtensorMap *map, const uint8_t *in, uint64_t n,
 cudaError_t index_launch(const IndexLaunch &L, const CUtensorMap *map,
                          bool use_tma, cudaStream_t stream,
                          int threads = kIndexThreads);
+
+// Launches the indexer for tiles [t0, t1) only, without touching the
+// scratch: the look-back descriptors of the tiles before t0 must already be
+// final (an earlier launch on the same stream), the ticket counter zero and
+// the rest of the descriptors clear (index_clear_scratch).  A file read in
+// pieces is indexed by one launch per piece as the pieces arrive.
+cudaError_t index_launch_range(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
+                               cudaStream_t stream, uint32_t t0, uint32_t t1,
+                               int threads = kIndexThreads);
+cudaError_t index_clear_scratch(const IndexLaunch &L, cudaStream_t stream);
+cudaError_t index_clear_counter(const IndexLaunch &L, cudaStream_t stream);
 
 inline uint64_t tiles_for(uint64_t n, int threads) {
   const uint64_t tb = uint64_t(threads) * 128u;

@@ -116,6 +116,54 @@ def test_query_host_end_to_end(cuda_ctx, gpj):
                                       want.query(c.ir_bytes, c.num_result_slots))
 
 
+def _pieces_input():
+    """About 73 MiB of post records with, at each 32 MiB boundary, a record
+    whose string holds a backslash run that ends right at the boundary, so
+    that the escape, string and depth carries cross the piece boundaries."""
+    from gpjson_b200 import datagen
+    piece = 32 << 20
+    out = bytearray()
+    for k, boundary in enumerate((piece, 2 * piece)):
+        rec = (b'{"a":"' + b"q" * 18 + b"\\\\\\" + b'"' + b"z" * 30 +
+               b'","user":{"lang":"b%d"}}\n' % k)
+        start = boundary - 27  # the quote after the three backslashes lands on the boundary
+        seg = datagen.tweets(20 + k, start - len(out) - 4096).tobytes()
+        seg = seg[: seg.rfind(b"\n") + 1]
+        out += seg
+        out += b" " * (start - len(out) - 1) + b"\n"
+        assert len(out) == start
+        out += rec
+    out += datagen.tweets(30, 9 << 20).tobytes()
+    return np.frombuffer(bytes(out), np.uint8).copy()
+
+
+def test_query_host_pieces(cuda_ctx, gpj):
+    """Host inputs of more than one 32 MiB piece are copied and indexed piece
+    by piece (the index of a piece overlaps the copy of the next); results
+    equal the oracle's on the whole input."""
+    data = _pieces_input()
+    assert data.size > (64 << 20) + (8 << 20)
+    comp = [gpj.compile(q) for q in ["$.user.lang", "$.a", "$.entities.hashtags[0:8].text"]]
+    L = max(c.max_depth for c in comp)
+    lines = data.tobytes().count(b"\n") + 1
+    host_in = torch.from_numpy(data).pin_memory()
+    outs = [torch.empty(lines * c.num_result_slots * 2, dtype=torch.int32).pin_memory()
+            for c in comp]
+    got_lines = cuda_ctx.query_host(host_in.data_ptr(), data.size, L, comp,
+                                    [o.data_ptr() for o in outs], [o.numel() for o in outs])
+    assert got_lines == lines
+    want = oracle.OracleIndex(data, L)
+    texts_seen = set()
+    for c, o in zip(comp, outs):
+        got = o.numpy().astype(np.int64).reshape(lines, -1, 2)
+        np.testing.assert_array_equal(got, want.query(c.ir_bytes, c.num_result_slots),
+                                      err_msg=c.query_text)
+        if c.query_text == "$.user.lang":
+            b = data.tobytes()
+            texts_seen = {b[s:e] for s, e in got[:, 0] if s >= 0}
+    assert b'"b0"' in texts_seen and b'"b1"' in texts_seen
+
+
 @pytest.mark.parametrize("query", ["$.categoryPath[1:3].id", "$.offers[0].type[1]", "$.sku",
                                    "$.categoryPath[*].name"])
 def test_array_element_records(cuda_ctx, gpj, query):
