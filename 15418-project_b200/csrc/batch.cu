@@ -58,6 +58,9 @@ struct gpj_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;
+  // gpj_batch_run_host: the input arrives in pieces on a copy stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t piece_ready = nullptr;
 };
 
 namespace {
@@ -146,6 +149,8 @@ void release(gpj_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->piece_ready) cudaEventDestroy(b->piece_ready);
+  if (b->copy_stream) cudaStreamDestroy(b->copy_stream);
   cudaFree(b->d_files);
   cudaFree(b->d_tile_file);
   cudaFree(b->d_tile_row);
@@ -464,17 +469,82 @@ int gpj_batch_run_per_file(gpj_batch *b, void *stream_) {
   return GPJ_OK;
 }
 
+namespace {
+
+// Host input of a batch: copied in pieces of whole files of about this many
+// bytes; the tiles of each piece are indexed as soon as it is on the device,
+// so indexing overlaps the copy of the next piece.  Finalize and queries run
+// once every piece is indexed.
+constexpr uint64_t kPieceBytes = uint64_t(32) << 20;
+
+// Pieces are byte ranges between file starts: the files must lie in table
+// order without overlapping (as gpjson_b200.pack_files lays them out).
+bool files_in_order(const gpj_batch *b) {
+  for (uint32_t f = 0; f + 1 < b->num_files; ++f)
+    if (b->files[f].in_off + b->files[f].n > b->files[f + 1].in_off) return false;
+  return true;
+}
+
+int run_in_pieces(gpj_batch *b, const uint8_t *h_input, cudaStream_t stream) {
+  if (b->copy_stream == nullptr)
+    BCUDA(cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (b->piece_ready == nullptr)
+    BCUDA(cudaEventCreateWithFlags(&b->piece_ready, cudaEventDisableTiming), "cudaEventCreate");
+  auto *d_in = const_cast<uint8_t *>(b->d_input);
+  const CUtensorMap *map = b->tma ? &b->map : nullptr;
+  BCUDA(gpjb::index_clear_scratch(b->L, stream), "cudaMemsetAsync");
+  // the copies start after the work already queued on `stream`
+  BCUDA(cudaEventRecord(b->piece_ready, stream), "cudaEventRecord");
+  BCUDA(cudaStreamWaitEvent(b->copy_stream, b->piece_ready, 0), "cudaStreamWaitEvent");
+  uint32_t f = 0;
+  while (f < b->num_files) {
+    // files [f, g): at least one, then more while the piece stays small
+    const uint64_t start = f == 0 ? 0u : b->files[f].in_off;
+    uint32_t g = f + 1;
+    while (g < b->num_files && b->files[g].in_off + b->files[g].n - start <= kPieceBytes) ++g;
+    const uint64_t end = g < b->num_files ? b->files[g].in_off : b->input_bytes;
+    const uint32_t t0 = b->files[f].first_tile;
+    const uint32_t t1 = g < b->num_files ? b->files[g].first_tile : b->L.num_tiles;
+    if (end > start)
+      BCUDA(cudaMemcpyAsync(d_in + start, h_input + start, end - start, cudaMemcpyHostToDevice,
+                            b->copy_stream),
+            "copy batch input piece");
+    BCUDA(cudaEventRecord(b->piece_ready, b->copy_stream), "cudaEventRecord");
+    BCUDA(cudaStreamWaitEvent(stream, b->piece_ready, 0), "cudaStreamWaitEvent");
+    if (t1 > t0) {
+      BCUDA(gpjb::index_clear_counter(b->L, stream), "cudaMemsetAsync");
+      BCUDA(gpjb::index_launch_range(b->L, map, b->tma, stream, t0, t1, b->index_threads),
+            "index kernel launch");
+    }
+    f = g;
+  }
+  BCUDA(gpjb::index_finalize_files(b->L, b->d_query_of_file, b->d_slots, b->d_info,
+                                   b->d_totals, stream),
+        "finalize launch");
+  BCUDA(gpjb::batch_query_launch(query_launch_of(b), b->blob, b->query_grid, b->query_block,
+                                 stream),
+        "batch query launch");
+  return GPJ_OK;
+}
+
+}  // namespace
+
 int gpj_batch_run_host(gpj_batch *b, const uint8_t *h_input, int32_t *h_results,
                        uint64_t *h_file_info, void *stream_) {
   if (b == nullptr || h_input == nullptr)
     return gpjb::report_error(GPJ_ERR_INVALID_ARGUMENT, "null batch or input");
   auto stream = static_cast<cudaStream_t>(stream_);
   BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
-  BCUDA(cudaMemcpyAsync(const_cast<uint8_t *>(b->d_input), h_input, b->input_bytes,
-                        cudaMemcpyHostToDevice, stream),
-        "copy batch input");
-  const int rc = gpj_batch_run(b, stream_);
-  if (rc != GPJ_OK) return rc;
+  if (b->input_bytes <= kPieceBytes || b->L.num_tiles == 0 || !files_in_order(b)) {
+    BCUDA(cudaMemcpyAsync(const_cast<uint8_t *>(b->d_input), h_input, b->input_bytes,
+                          cudaMemcpyHostToDevice, stream),
+          "copy batch input");
+    const int rc = gpj_batch_run(b, stream_);
+    if (rc != GPJ_OK) return rc;
+  } else {
+    const int rc = run_in_pieces(b, h_input, stream);
+    if (rc != GPJ_OK) return rc;
+  }
   if (h_results != nullptr && b->result_ints > 0)
     BCUDA(cudaMemcpyAsync(h_results, b->d_out, b->result_ints * 4u, cudaMemcpyDeviceToHost,
                           stream),

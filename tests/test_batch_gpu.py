@@ -138,3 +138,42 @@ def test_plain_per_file_launches_match_batch(gpj):
                                              (v.d_leveled, v.leveled_words, np.uint64)]]
     for g, w in zip(got, want):
         np.testing.assert_array_equal(g, w)
+
+
+def test_batch_run_host_in_pieces(gpj):
+    """gpj_batch_run_host on more than one 32 MiB piece: the packed files are
+    copied piece by piece and each piece is indexed as soon as it lands.  The
+    device buffer starts out as garbage, so a piece indexed before its bytes
+    arrived would show; every file must still equal the oracle."""
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    from gpjson_b200 import datagen
+    files = _files(4, 30)
+    files.insert(7, (bytes(datagen.tweets(41, 40 << 20)), 0))
+    files.insert(15, (bytes(datagen.products(42, 20 << 20)), 1))
+    files += [(bytes(datagen.tweets(43 + i, 300000)), 0) for i in range(20)]
+    comp = [(gpj.compile(q), base) for q, base in QUERIES]
+    queries = [(c, base, c.max_depth + base) for c, base in comp]
+    buf, offsets = gpj.pack_files([d for d, _ in files])
+    assert buf.size > (64 << 20)
+    dev = torch.from_numpy(buf).cuda()  # creation sizes the outputs on the real bytes
+    host = torch.from_numpy(buf).pin_memory()
+    table = [(o, len(d), k) for o, (d, k) in zip(offsets, files)]
+    with gpj.Batch(dev.data_ptr(), buf.size, table, queries) as b:
+        v = b.view()
+        dev.fill_(ord("{"))
+        torch.cuda.synchronize()
+        results = torch.empty(max(1, v.result_ints), dtype=torch.int32).pin_memory()
+        info = torch.empty(v.num_files * gpj.FILE_INFO_WORDS, dtype=torch.int64).pin_memory()
+        b.run_host(host.data_ptr(), results.data_ptr(), info.data_ptr())
+        got = {
+            "info": info.numpy().view(np.uint64).reshape(-1, 8),
+            "totals": d2h(v.d_totals, 4, np.uint64),
+            "S": d2h(v.d_string, v.string_words, np.uint64),
+            "LB": d2h(v.d_leveled, v.leveled_words, np.uint64),
+            "NL": d2h(v.d_newline, v.newline_slots, np.int64),
+            "R": results.numpy()[:v.result_ints],
+            "layout": [b.file_layout(f) for f in range(len(files))],
+        }
+    assert torch.equal(dev.cpu(), torch.from_numpy(buf))
+    _check(files, comp, queries, got)
