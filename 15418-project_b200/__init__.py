@@ -20,6 +20,8 @@ import ctypes as C
 from dataclasses import dataclass
 from pathlib import Path
 
+import numpy as np
+
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "lib" / "libgpjson_b200.so"
 
@@ -46,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_build_noalloc",
     "gpj_index_free",
     "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
+    "gpj_results_compact",
     "gpj_batch_create", "gpj_batch_run", "gpj_batch_run_stages", "gpj_batch_run_per_file",
     "gpj_batch_run_host",
     "gpj_batch_view_get", "gpj_batch_file_layout", "gpj_batch_destroy",
@@ -229,6 +232,8 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_query_run64.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
     lib.gpj_query_run_opts.argtypes = [vp, P(Index), vp, u64, u32, P(QueryOpts), vp, vp]
     lib.gpj_query_host.argtypes = [vp, vp, u64, i32, u32, vp, vp, vp, vp, vp, vp, P(u64), vp]
+    lib.gpj_results_compact.argtypes = [vp, vp, u64, u32, vp, u64, C.c_int64, vp, u64, vp, u64,
+                                        vp, vp]
     lib.gpj_batch_create.argtypes = [vp, vp, u64, P(BatchFile), u32, P(BatchQuery), u32, u32,
                                      P(vp), vp]
     lib.gpj_batch_run.argtypes = [vp, vp]
@@ -362,6 +367,15 @@ class Context:
                                             compiled.num_result_slots, C.byref(opts),
                                             C.c_void_p(d_out), C.c_void_p(stream)))
 
+    def compact(self, d_results: int, num_lines: int, num_result_slots: int, d_input: int,
+                size_bytes: int, base_offset: int, d_matches: int, match_capacity: int,
+                d_arena: int, arena_capacity: int, d_counts: int, stream: int = 0) -> None:
+        """gpj_results_compact: device pointers in, asynchronous on `stream`."""
+        _check(self._lib.gpj_results_compact(
+            self._h, C.c_void_p(d_results), num_lines, num_result_slots, C.c_void_p(d_input),
+            size_bytes, base_offset, C.c_void_p(d_matches), match_capacity, C.c_void_p(d_arena),
+            arena_capacity, C.c_void_p(d_counts), C.c_void_p(stream)))
+
     def query_host(self, h_input: int, size_bytes: int, num_levels: int,
                    compiled: list[CompiledQuery], h_outs: list[int],
                    capacities: list[int], stream: int = 0,
@@ -381,6 +395,42 @@ class Context:
                                         q, ir_ptrs, ir_lens, slots, bases, outs, caps,
                                         C.byref(lines), C.c_void_p(stream)))
         return lines.value
+
+
+# gpj_match as a numpy record (40 bytes)
+MATCH_DTYPE = np.dtype([("line", "<u8"), ("slot", "<u4"), ("length", "<u4"),
+                        ("start", "<i8"), ("end", "<i8"), ("text_offset", "<u8")])
+
+
+def compact_results(ctx: "Context", d_results: int, num_lines: int, num_result_slots: int,
+                    d_input: int, size_bytes: int, base_offset: int = 0,
+                    match_capacity: int = 1 << 16, arena_capacity: int = 1 << 20,
+                    stream: int = 0):
+    """Compacts one query's device result array on the device
+    (gpj_results_compact) and copies back only the matches and their bytes.
+    Returns (matches as a MATCH_DTYPE array, arena bytes); raises
+    QueryExecutionError for an invalid range as the reference does.  Device
+    buffers are torch allocations, grown and the call repeated when the
+    first guess of the capacities is too small."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    counts = torch.zeros(3, dtype=torch.int64, device=dev)
+    while True:
+        matches = torch.empty(max(1, match_capacity) * MATCH_DTYPE.itemsize, dtype=torch.uint8,
+                              device=dev)
+        arena = torch.empty(max(1, arena_capacity), dtype=torch.uint8, device=dev)
+        ctx.compact(d_results, num_lines, num_result_slots, d_input, size_bytes, base_offset,
+                    matches.data_ptr(), match_capacity, arena.data_ptr(), arena_capacity,
+                    counts.data_ptr(), stream)
+        torch.cuda.synchronize(dev)
+        m, nbytes, invalid = (int(x) for x in counts.cpu())
+        if invalid:
+            raise QueryExecutionError("Query kernel produced an invalid result range")
+        if m <= match_capacity and nbytes <= arena_capacity:
+            break
+        match_capacity, arena_capacity = max(m, 1), max(nbytes, 1)
+    out = matches[: m * MATCH_DTYPE.itemsize].cpu().numpy().view(MATCH_DTYPE)
+    return out, bytes(arena[:nbytes].cpu().numpy())
 
 
 def pack_files(files, align: int = 128):

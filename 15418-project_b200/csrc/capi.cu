@@ -2,6 +2,7 @@
 // buffer reuse, launches and error reporting.  No CPU fallback: every entry
 // point that computes needs a CUDA device and fails with GPJ_ERR_CUDA
 // otherwise.
+#include "compact.cuh"
 #include "compiler.hpp"
 #include "indexer.cuh"
 #include "query.cuh"
@@ -25,6 +26,8 @@ struct gpj_ctx {
   void *host_results = nullptr;
   uint64_t host_results_bytes = 0;
   unsigned long long *pinned = nullptr;  // 8 words of pinned host memory
+  void *compact_scratch = nullptr;  // per-block counts of gpj_results_compact
+  uint64_t compact_scratch_bytes = 0;
   // host inputs arrive in pieces on a copy stream (created on first use)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t piece_ready = nullptr;
@@ -342,6 +345,7 @@ int gpj_ctx_destroy(gpj_ctx *ctx) {
   cudaFree(ctx->staging);
   cudaFree(ctx->host_index);
   cudaFree(ctx->host_results);
+  cudaFree(ctx->compact_scratch);
   cudaFreeHost(ctx->pinned);
   if (ctx->piece_ready) cudaEventDestroy(ctx->piece_ready);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -548,6 +552,32 @@ int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes, in
     return GPJ_OK;
   }
   return fail(GPJ_ERR_IMPLEMENTATION, "newline capacity retry failed");
+}
+
+int gpj_results_compact(gpj_ctx *ctx, const int32_t *d_results, uint64_t num_lines,
+                        uint32_t num_result_slots, const uint8_t *d_input, uint64_t size_bytes,
+                        int64_t base_offset, gpj_match *d_matches, uint64_t match_capacity,
+                        uint8_t *d_arena, uint64_t arena_capacity, uint64_t *d_counts,
+                        void *stream_) {
+  int rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  if (d_counts == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null counts");
+  const uint64_t items = num_lines * uint64_t(num_result_slots);
+  if (items > 0 && d_results == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null results");
+  if (match_capacity > 0 && d_matches == nullptr)
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "null match buffer");
+  if (num_result_slots > 0 && num_lines > UINT64_MAX / num_result_slots / 2u)
+    return fail(GPJ_ERR_OUT_OF_RANGE, "result array too large");
+  rc = ensure(ctx->compact_scratch, ctx->compact_scratch_bytes,
+              gpjb::compact_scratch_bytes(num_lines, num_result_slots));
+  if (rc != GPJ_OK) return rc;
+  GPJ_CUDA(gpjb::compact_launch(d_results, num_lines, num_result_slots, d_input, size_bytes,
+                                base_offset, d_matches, match_capacity, d_arena,
+                                arena_capacity,
+                                reinterpret_cast<unsigned long long *>(d_counts),
+                                ctx->compact_scratch, static_cast<cudaStream_t>(stream_)),
+           "result compaction launch");
+  return GPJ_OK;
 }
 
 }  // extern "C"

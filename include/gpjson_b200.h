@@ -176,6 +176,35 @@ int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes,
                    int32_t *const *h_out, const uint64_t *out_capacity,
                    uint64_t *num_lines, void *stream);
 
+/* One match of a compacted result array (gpj_results_compact). */
+typedef struct gpj_match {
+  uint64_t line;         /* record (line) index */
+  uint32_t slot;         /* result slot of the query */
+  uint32_t length;       /* end - start */
+  int64_t start;         /* global byte offset: base_offset + partition-local start */
+  int64_t end;           /* global end offset, exclusive */
+  uint64_t text_offset;  /* first byte of the match in the arena */
+} gpj_match;
+
+/* Compacts one query's int32 result array d_results[num_lines][slots][2]
+ * (partition-local, -1 = no match) on the device: the matches in (line,
+ * slot) order with global offsets into d_matches, and the matched bytes of
+ * d_input, concatenated in the same order, into d_arena.  d_counts (3
+ * words, device) receives the number of matches, the arena bytes they need
+ * and the number of invalid ranges (start > end or end > size_bytes, which
+ * the reference reports as "Query kernel produced an invalid result range").
+ * Matches and bytes beyond match_capacity / arena_capacity are counted but
+ * not written: call again with larger buffers.  d_arena or d_input may be
+ * NULL (offsets only).  Asynchronous on `stream`.  Replaces the host loop of
+ * append_query_line_results (src/gpjson/query/kernels/orig/
+ * query_executor_host.cu:80-119): only the matches and their bytes need to
+ * be copied to the host. */
+int gpj_results_compact(gpj_ctx *ctx, const int32_t *d_results, uint64_t num_lines,
+                        uint32_t num_result_slots, const uint8_t *d_input,
+                        uint64_t size_bytes, int64_t base_offset, gpj_match *d_matches,
+                        uint64_t match_capacity, uint8_t *d_arena, uint64_t arena_capacity,
+                        uint64_t *d_counts, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Batched path: many files indexed and queried by one launch chain         */
 /* ------------------------------------------------------------------------ */
