@@ -402,6 +402,22 @@ def barrier(world: int):
         dist.barrier()
 
 
+INT32_MAX = 0x7FFFFFFF
+
+
+def newline_partitions(data, limit: int):
+    """[start, end) byte ranges below `limit` bytes, cut after a newline that
+    is left out of both sides (reference file_reader.cpp:65-66)."""
+    n = int(data.size)
+    parts, start = [], 0
+    while n - start > limit:
+        cut = start + int(np.flatnonzero(data[start:start + limit] == 10)[-1])
+        parts.append((start, cut))
+        start = cut + 1
+    parts.append((start, n))
+    return parts
+
+
 def algorithmic_index_bytes(n: int, levels: int, lines: int) -> int:
     # input read once + S + L leveled words + newline index (int64)
     W = (n + 63) // 64
@@ -440,25 +456,31 @@ def run_ours(args, world, rank, local):
     lines = int(summ[0].item())
     assert lines <= nl_cap and int(summ[3].item()) == 0
     ix.num_lines = lines
-    outs = [torch.empty(lines * c.num_result_slots * 2, dtype=torch.int32, device=dev)
+    # partitions of 2 GiB and more need int64 offsets (the reference's int
+    # results stop below 2 GiB, query_executor_host.cu:28-33)
+    wide = n > INT32_MAX
+    outs = [torch.empty(lines * c.num_result_slots * 2,
+                        dtype=torch.int64 if wide else torch.int32, device=dev)
             for c, _ in comp]
 
     def step(ev=None):
+        # ev: [start, index done, query 0 done, query 1 done, ...]
         if ev is not None:
             ev[0].record(stream)
         ctx.build_index_async(d_in.data_ptr(), n, levels, ix, summ.data_ptr(), stream=s)
         if ev is not None:
             ev[1].record(stream)
-        for (c, base), o in zip(comp, outs):
-            ctx.query(ix, c, o.data_ptr(), stream=s, base_level=base)
-        if ev is not None:
-            ev[2].record(stream)
+        for q, ((c, base), o) in enumerate(zip(comp, outs)):
+            ctx.query(ix, c, o.data_ptr(), stream=s, base_level=base, wide=wide)
+            if ev is not None:
+                ev[2 + q].record(stream)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
     stream.synchronize()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2 + len(comp))]
+           for _ in range(args.steps)]
     clocks = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize(dev)
@@ -470,33 +492,52 @@ def run_ours(args, world, rank, local):
                 flush.fill_(k)
             step(evs[k])
     torch.cuda.synchronize(dev)
+    t_query = [0.0] * len(comp)
     for e in evs:
         t_index += e[0].elapsed_time(e[1])
-        t_total += e[0].elapsed_time(e[2])
+        t_total += e[0].elapsed_time(e[-1])
+        for q in range(len(comp)):
+            t_query[q] += e[1 + q].elapsed_time(e[2 + q])
     barrier(world)
     clk = clocks.stop()
     ms_step = allreduce_max(t_total / args.steps, world)
     ms_index = allreduce_max(t_index / args.steps, world)
+    ms_query = [allreduce_max(t / args.steps, world) for t in t_query]
 
-    # end to end through the host-buffer C ABI call
+    # end to end through the host-buffer C ABI call, one call per partition
+    # (partitions below 2 GiB split at newlines, as the reference's engine
+    # cuts files; a single partition for every input below 2 GiB)
     h_in = torch.from_numpy(data).pin_memory()
-    h_outs = [torch.empty(o.numel(), dtype=torch.int32).pin_memory() for o in outs]
+    parts = newline_partitions(data, INT32_MAX)
+    h_outs = []  # per partition, per query
+    for p0, p1 in parts:
+        pl = int(np.count_nonzero(data[p0:p1] == 10)) + 1
+        h_outs.append([torch.empty(pl * c.num_result_slots * 2, dtype=torch.int32).pin_memory()
+                       for c, _ in comp])
     e2e_ms = []
     for k in range(args.warmup + args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        got = ctx.query_host(h_in.data_ptr(), n, levels, [c for c, _ in comp],
-                             [h.data_ptr() for h in h_outs], [h.numel() for h in h_outs],
-                             stream=s, base_levels=[b for _, b in comp])
+        got = 0
+        for (p0, p1), hp in zip(parts, h_outs):
+            got += ctx.query_host(h_in.data_ptr() + p0, p1 - p0, levels, [c for c, _ in comp],
+                                  [h.data_ptr() for h in hp], [h.numel() for h in hp],
+                                  stream=s, base_levels=[b for _, b in comp])
         e1.record(stream)
         e1.synchronize()
         assert got == lines
         if k >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
-    # bit-exact check of the e2e results against the device-resident run
-    for h, o in zip(h_outs, outs):
-        assert torch.equal(h, o.cpu()), "e2e results differ from the device-resident run"
+    # bit-exact check of the e2e results against the device-resident run:
+    # partition-local offsets plus the partition start are the global ones
+    for q, o in enumerate(outs):
+        pieces = []
+        for (p0, _), hp in zip(parts, h_outs):
+            h = hp[q].numpy().astype(np.int64)
+            pieces.append(np.where(h >= 0, h + p0, h))
+        assert np.array_equal(np.concatenate(pieces), o.cpu().numpy().astype(np.int64)), \
+            "e2e results differ from the device-resident run"
 
     gb = n * world / 1e9
     peak, peak_kind = measured_peak_hbm()
@@ -519,8 +560,9 @@ def run_ours(args, world, rank, local):
                    "l2": "flushed between steps" if flush is not None else
                          "input larger than L2", "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(gb / (e2e_step / 1e3), 3), "unit": "GB/s",
-                "h2d_bytes_per_step": n,
-                "d2h_bytes_per_step": sum(h.numel() * 4 for h in h_outs)},
+                "h2d_bytes_per_step": sum(p1 - p0 for p0, p1 in parts),
+                "d2h_bytes_per_step": sum(h.numel() * 4 for hp in h_outs for h in hp),
+                "partitions": len(parts)},
         "gpu_launches": 1 + len(comp),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -528,6 +570,9 @@ def run_ours(args, world, rank, local):
                      "algorithmic_bytes_per_launch": b_index,
                      "ms_per_launch": round(ms_index, 4)},
         "index_ms": round(ms_index, 4), "query_ms": round(ms_step - ms_index, 4),
+        "index_gbs": round(n / 1e9 / (ms_index / 1e3), 1),
+        "per_query": [{"query": q, "ms": round(t, 4), "gbs": round(n / 1e9 / (t / 1e3), 1)}
+                      for q, t in zip(queries, ms_query)],
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
