@@ -611,12 +611,11 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
   uint32_t pex = uint32_t(__popc(par_ballot & lt_mask)) & 1u;
   if (lane == 0) sm.warp_par[warp] = uint32_t(__popc(par_ballot)) & 1u;
   compute_sync<NT>();  // (2)
-  uint32_t tile_par = 0;
-#pragma unroll
-  for (int w = 0; w < NWARPS; ++w) {
-    if (w < warp) pex ^= sm.warp_par[w];
-    tile_par ^= sm.warp_par[w];
-  }
+  // the warps' parities as one bit mask (lane w reads warp w's)
+  const uint32_t wpar =
+      __ballot_sync(0xFFFFFFFFu, lane < NWARPS && sm.warp_par[lane < NWARPS ? lane : 0] != 0u);
+  pex ^= uint32_t(__popc(wpar & ((1u << warp) - 1u))) & 1u;
+  const uint32_t tile_par = uint32_t(__popc(wpar)) & 1u;
   // depth changes are only needed mod 256: two 16-bit lanes cannot overflow
   // over at most 256 threads (256 * 255 < 65536)
   const int dt0 = pex ? (thr_t - thr_d0) : thr_d0;
@@ -636,17 +635,25 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
     sm.warp_nl[warp] = nl_inc;
   }
   compute_sync<NT>();  // (3)
-  uint32_t dd_ex = dd_inc - dd, nl_ex = nl_inc - thr_nl;
-  uint32_t tile_dd = 0, tile_nl = 0;
+  // inclusive scan of the warps' sums over lanes 0 .. NWARPS-1
+  uint32_t wdd = lane < NWARPS ? sm.warp_dd[lane < NWARPS ? lane : 0] : 0u;
+  uint32_t wnl = lane < NWARPS ? sm.warp_nl[lane < NWARPS ? lane : 0] : 0u;
 #pragma unroll
-  for (int w = 0; w < NWARPS; ++w) {
-    if (w < warp) {
-      dd_ex += sm.warp_dd[w];
-      nl_ex += sm.warp_nl[w];
+  for (int off = 1; off < NWARPS; off <<= 1) {
+    const uint32_t a = __shfl_up_sync(0xFFFFFFFFu, wdd, off);
+    const uint32_t b = __shfl_up_sync(0xFFFFFFFFu, wnl, off);
+    if (lane >= off) {
+      wdd += a;
+      wnl += b;
     }
-    tile_dd += sm.warp_dd[w];
-    tile_nl += sm.warp_nl[w];
   }
+  const int prev_warp = warp > 0 ? warp - 1 : 0;
+  const uint32_t before_dd = __shfl_sync(0xFFFFFFFFu, wdd, prev_warp);
+  const uint32_t before_nl = __shfl_sync(0xFFFFFFFFu, wnl, prev_warp);
+  const uint32_t tile_dd = __shfl_sync(0xFFFFFFFFu, wdd, NWARPS - 1);
+  const uint32_t tile_nl = __shfl_sync(0xFFFFFFFFu, wnl, NWARPS - 1);
+  const uint32_t dd_ex = dd_inc - dd + (warp > 0 ? before_dd : 0u);
+  const uint32_t nl_ex = nl_inc - thr_nl + (warp > 0 ? before_nl : 0u);
   if (tid == 0) {
     // publish the aggregate at once: look-backs of later tiles wait for it
     if (tile != 0)
