@@ -411,7 +411,11 @@ def newline_partitions(data, limit: int):
     n = int(data.size)
     parts, start = [], 0
     while n - start > limit:
-        cut = start + int(np.flatnonzero(data[start:start + limit] == 10)[-1])
+        nls = np.flatnonzero(data[start:start + limit] == 10)
+        if nls.size == 0:
+            raise ValueError(f"no newline within {limit} bytes of offset {start}: "
+                             "a record longer than a partition")
+        cut = start + int(nls[-1])
         parts.append((start, cut))
         start = cut + 1
     parts.append((start, n))
