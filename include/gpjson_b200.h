@@ -165,10 +165,14 @@ int gpj_query_run_opts(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir
 
 /* End to end from host memory: copies h_input to the device, builds the
  * index with num_levels levels, runs the queries and copies the int32 result
- * arrays back.  h_out[q] must hold out_capacity[q] int32; *num_lines gets
- * the record count (0 for an empty input).  base_levels may be NULL (all 0).  GPJ_ERR_CAPACITY (nothing copied back) if a result does
- * not fit.  Replaces the per-partition body of gpjson::Engine::query
- * (src/gpjson/engine.cpp:131-166: load_to_device, build, execute_batch). */
+ * arrays back.  Inputs above 32 MiB are copied in pieces on a second stream
+ * and each piece is indexed as soon as it is on the device (pinned host
+ * memory makes the copies overlap the indexing).  h_out[q] must hold
+ * out_capacity[q] int32; *num_lines gets the record count (0 for an empty
+ * input).  base_levels may be NULL (all 0).  GPJ_ERR_CAPACITY (nothing
+ * copied back) if a result does not fit.  Replaces the per-partition body
+ * of gpjson::Engine::query (src/gpjson/engine.cpp:131-166: load_to_device,
+ * build, execute_batch). */
 int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes,
                    int num_levels, uint32_t num_queries,
                    const uint8_t *const *h_irs, const uint64_t *ir_lens,
@@ -293,7 +297,10 @@ int gpj_batch_run_per_file(gpj_batch *batch, void *stream);
 /* End to end from host memory: copies h_input (input_bytes, the batch's
  * layout) into the batch's device input buffer, runs the batch, copies the
  * result ints (view.result_ints) and the per-file info (8 uint64 per file)
- * back, and waits.  Either output pointer may be NULL. */
+ * back, and waits.  Either output pointer may be NULL.  Above 32 MiB, with
+ * the files in table order and not overlapping, the input is copied in
+ * groups of whole files and each group is indexed as soon as it lands; the
+ * finalize and the queries follow the last group. */
 int gpj_batch_run_host(gpj_batch *batch, const uint8_t *h_input, int32_t *h_results,
                        uint64_t *h_file_info, void *stream);
 
