@@ -39,6 +39,8 @@ GPJ_ERR_IMPLEMENTATION = 10
 
 GPJ_INDEX_EMIT_ESCAPE_QUOTE = 1
 GPJ_INDEX_NO_TMA = 2
+GPJ_INDEX_DIAG_TILE0_UNPUBLISHED = 0x80000000
+GPJ_QUERY_OVERFLOW = 0x100  # a record had more results than result slots
 MAX_LEVELS = 22
 MAX_QUERY_IR = 4096
 MAX_QUERY_DEPTH = 16
@@ -48,6 +50,7 @@ EXPORTED_SYMBOLS = (
     "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_build_noalloc",
     "gpj_index_free",
     "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
+    "gpj_query_status",
     "gpj_results_compact",
     "gpj_batch_create", "gpj_batch_run", "gpj_batch_run_stages", "gpj_batch_run_per_file",
     "gpj_batch_run_host",
@@ -232,6 +235,7 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_query_run64.argtypes = [vp, P(Index), vp, u64, u32, vp, vp]
     lib.gpj_query_run_opts.argtypes = [vp, P(Index), vp, u64, u32, P(QueryOpts), vp, vp]
     lib.gpj_query_host.argtypes = [vp, vp, u64, i32, u32, vp, vp, vp, vp, vp, vp, P(u64), vp]
+    lib.gpj_query_status.argtypes = [vp, P(u32), vp]
     lib.gpj_results_compact.argtypes = [vp, vp, u64, u32, vp, u64, C.c_int64, vp, u64, vp, u64,
                                         vp, vp]
     lib.gpj_batch_create.argtypes = [vp, vp, u64, P(BatchFile), u32, P(BatchQuery), u32, u32,
@@ -366,6 +370,13 @@ class Context:
         _check(self._lib.gpj_query_run_opts(self._h, C.byref(index), ir, len(compiled.ir_bytes),
                                             compiled.num_result_slots, C.byref(opts),
                                             C.c_void_p(d_out), C.c_void_p(stream)))
+
+    def query_status(self, stream: int = 0) -> int:
+        """gpj_query_status: status bits of this context's queries since the
+        last call (GPJ_QUERY_OVERFLOW), cleared by the call."""
+        flags = C.c_uint32()
+        _check(self._lib.gpj_query_status(self._h, C.byref(flags), C.c_void_p(stream)))
+        return flags.value
 
     def compact(self, d_results: int, num_lines: int, num_result_slots: int, d_input: int,
                 size_bytes: int, base_offset: int, d_matches: int, match_capacity: int,

@@ -128,6 +128,9 @@ gpjb::BatchQueryLaunch query_launch_of(const gpj_batch *b) {
   q.file_info = b->d_info;
   q.totals = b->d_totals;
   q.out = b->d_out;
+  // overflow of extension queries lands in the error word of the totals
+  // (written by the finalize kernel just before the query launch)
+  q.status = reinterpret_cast<unsigned int *>(b->d_totals + gpjb::kTotError);
   q.num_groups = int(b->groups.size());
   for (size_t g = 0; g < b->groups.size(); ++g) q.groups[g] = b->groups[g];
   return q;
@@ -462,6 +465,7 @@ int gpj_batch_run_per_file(gpj_batch *b, void *stream_) {
     q.num_levels = F.levels;
     q.base_level = G.base_level;
     q.out32 = b->d_out + row[gpjb::kFiOutOff];
+    q.status = reinterpret_cast<unsigned int *>(b->d_totals + gpjb::kTotError);
     gpjb::IrBlob blob;
     std::memcpy(blob.bytes, b->blob.bytes + G.ir_off, size_t(G.ir_len));
     BCUDA(gpjb::query_launch(q, blob, 0, 256, stream), "per-file query launch");
@@ -553,7 +557,16 @@ int gpj_batch_run_host(gpj_batch *b, const uint8_t *h_input, int32_t *h_results,
     BCUDA(cudaMemcpyAsync(h_file_info, b->d_info, uint64_t(b->num_files) * 64u,
                           cudaMemcpyDeviceToHost, stream),
           "copy batch file info");
+  uint64_t err = 0;
+  BCUDA(cudaMemcpyAsync(&err, b->d_totals + gpjb::kTotError, 8, cudaMemcpyDeviceToHost, stream),
+        "copy batch error word");
   BCUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+  if (err & (gpjb::kErrLookbackTimeout | gpjb::kErrTmaTimeout | gpjb::kErrPipelineTimeout))
+    return gpjb::report_error(GPJ_ERR_TIMEOUT, "batch index: a bounded device wait gave up");
+  if (err & gpjb::kQueryStatusOverflow)
+    return gpjb::report_error(GPJ_ERR_CAPACITY,
+                              "batch query: a record has more results than result slots; the "
+                              "results are truncated");
   return GPJ_OK;
 }
 

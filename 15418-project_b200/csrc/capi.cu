@@ -31,6 +31,8 @@ struct gpj_ctx {
   // host inputs arrive in pieces on a copy stream (created on first use)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t piece_ready = nullptr;
+  // status bits the context's query launches raise (GPJ_QUERY_OVERFLOW)
+  unsigned int *d_status = nullptr;
 };
 
 namespace {
@@ -124,6 +126,16 @@ int enqueue_index(gpj_ctx *ctx, const uint8_t *in, uint64_t n, int levels,
              "summary");
     if (out.newline_capacity > 0)
       GPJ_CUDA(cudaMemsetAsync(out.d_newline, 0, sizeof(int64_t), stream), "cudaMemsetAsync");
+    return GPJ_OK;
+  }
+  if (flags & GPJ_INDEX_DIAG_TILE0_UNPUBLISHED) {
+    if (L.num_tiles < 2)
+      return fail(GPJ_ERR_INVALID_ARGUMENT,
+                  "GPJ_INDEX_DIAG_TILE0_UNPUBLISHED needs an input of at least two tiles");
+    L.lookback_spin_limit = 1u << 14;
+    GPJ_CUDA(gpjb::index_clear_scratch(L, stream), "cudaMemsetAsync");
+    GPJ_CUDA(gpjb::index_launch_range(L, tma ? &map : nullptr, tma, stream, 1u, L.num_tiles),
+             "index kernel launch");
     return GPJ_OK;
   }
   GPJ_CUDA(gpjb::index_launch(L, tma ? &map : nullptr, tma, stream), "index kernel launch");
@@ -295,6 +307,7 @@ int run_query(gpj_ctx *ctx, const gpj_index *ix, const uint8_t *h_ir, uint64_t i
   q.num_levels = ix->num_levels;
   if constexpr (sizeof(OutT) == 8) q.out64 = reinterpret_cast<int64_t *>(d_out);
   else q.out32 = reinterpret_cast<int32_t *>(d_out);
+  q.status = ctx->d_status;
   gpjb::IrBlob blob;
   std::memset(blob.bytes, 0, sizeof(blob.bytes));
   std::memcpy(blob.bytes, h_ir, size_t(ir_len));
@@ -334,7 +347,30 @@ int gpj_ctx_create(int device, gpj_ctx **out) {
     return cuda_fail(pe, "cudaMallocHost");
   }
   ctx->pinned = static_cast<unsigned long long *>(pinned);
+  void *status = nullptr;
+  cudaError_t se = cudaMalloc(&status, 256);
+  if (se == cudaSuccess) se = cudaMemset(status, 0, 256);
+  if (se != cudaSuccess) {
+    cudaFree(status);
+    cudaFreeHost(pinned);
+    delete ctx;
+    return cuda_fail(se, "cudaMalloc");
+  }
+  ctx->d_status = static_cast<unsigned int *>(status);
   *out = ctx;
+  return GPJ_OK;
+}
+
+int gpj_query_status(gpj_ctx *ctx, uint32_t *flags, void *stream_) {
+  if (flags == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null flags");
+  int rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  auto stream = static_cast<cudaStream_t>(stream_);
+  auto *h = reinterpret_cast<unsigned int *>(ctx->pinned + 6);
+  GPJ_CUDA(cudaMemcpyAsync(h, ctx->d_status, 4, cudaMemcpyDeviceToHost, stream), "read status");
+  GPJ_CUDA(cudaMemsetAsync(ctx->d_status, 0, 4, stream), "clear status");
+  GPJ_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+  *flags = *h;
   return GPJ_OK;
 }
 
@@ -346,6 +382,7 @@ int gpj_ctx_destroy(gpj_ctx *ctx) {
   cudaFree(ctx->host_index);
   cudaFree(ctx->host_results);
   cudaFree(ctx->compact_scratch);
+  cudaFree(ctx->d_status);
   cudaFreeHost(ctx->pinned);
   if (ctx->piece_ready) cudaEventDestroy(ctx->piece_ready);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -536,6 +573,7 @@ int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes, in
     }
     rc = ensure(ctx->host_results, ctx->host_results_bytes, total);
     if (rc != GPJ_OK) return rc;
+    GPJ_CUDA(cudaMemsetAsync(ctx->d_status, 0, 4, stream), "clear status");
     uint64_t off = 0;
     for (uint32_t q = 0; q < num_queries; ++q) {
       auto *d_out = reinterpret_cast<int32_t *>(static_cast<unsigned char *>(ctx->host_results) + off);
@@ -548,7 +586,14 @@ int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes, in
                  "copy results");
       off += round256(need * 4u);
     }
+    auto *h_status = reinterpret_cast<unsigned int *>(ctx->pinned + 6);
+    GPJ_CUDA(cudaMemcpyAsync(h_status, ctx->d_status, 4, cudaMemcpyDeviceToHost, stream),
+             "read status");
     GPJ_CUDA(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    if (*h_status & GPJ_QUERY_OVERFLOW)
+      return fail(GPJ_ERR_CAPACITY,
+                  "a record has more results than result slots (a \"[*]\" array longer than "
+                  "the wildcard limit, or more \"..\" matches); the results are truncated");
     return GPJ_OK;
   }
   return fail(GPJ_ERR_IMPLEMENTATION, "newline capacity retry failed");

@@ -5,9 +5,17 @@
 // over "$", ".name", "['name']", "[i]", "[i,j,...]", "[a:b]", "[:b]", "[-i]",
 // "[-i:]" and "[?(@ == "x")]", emitting LEB128 operands
 // (query_compiler.cpp:20-26) and counting result slots and levels the same
-// way.  One extension, off unless asked for: with a wildcard limit K > 0,
-// "[*]" compiles exactly like "[0:K]" (the reference rejects "[*]",
-// query_compiler.cpp:287-289).
+// way.  Queries in the reference's syntax compile to the reference's IR byte
+// for byte.  Extensions (the reference rejects all of them):
+//  * "[*]" with a wildcard limit K > 0: an element-count check (opcode 0x0C,
+//    raises the overflow status when the array holds more than K elements)
+//    followed by exactly the IR of "[0:K]" (query_compiler.cpp:287-289);
+//  * "..name" as the last step, with a wildcard limit K > 0: every member
+//    named `name` inside the current value at any indexed level, in document
+//    order, into K result slots (opcode 0x0B; query_compiler.cpp:202-204);
+//  * numeric filters "[?(@<path> <op> <number>)]" with op one of == != < <=
+//    > >= (opcode 0x0A: exact decimal comparison), and "!=" ... the filter
+//    of the reference takes only == "string" (query_compiler.cpp:366-391).
 #include "compiler.hpp"
 
 #include <algorithm>
@@ -28,7 +36,17 @@ enum Op : uint8_t {
   kMark = 7,
   kReset = 8,
   kStringEquals = 9,
+  kNumberCompare = 10,  // extension: cmp byte, varint length, number text
+  kDescendKey = 11,     // extension: varint length, key bytes
+  kExpectAtMost = 12,   // extension: varint element limit
 };
+
+// Comparators of kNumberCompare.
+enum Cmp : uint8_t { kEq = 0, kNe = 1, kLt = 2, kLe = 3, kGt = 4, kGe = 5 };
+
+// Levels a "..name" query asks the index for: every level the executor
+// allows (max_depth < kMaxQueryLevels, query_executor_host.cu:129-131).
+constexpr uint64_t kDescendLevels = 15;
 
 class Emitter {
  public:
@@ -111,7 +129,7 @@ class Parser {
   CompiledIr run() {
     cur.expect('$');
     next_expression();
-    ir.store();
+    if (!descended) ir.store();  // "..name" stores its own matches
     ir.op(kEnd);
     CompiledIr out;
     out.ir = std::move(ir.bytes);
@@ -127,13 +145,24 @@ class Parser {
     case '.': dot(); break;
     case '[': bracket(); break;
     case ' ': return;
+    case '=':
+    case '!':
+    case '<':
+    case '>':
+      if (in_filter > 0) return;  // the comparison of a filter follows its path
+      [[fallthrough]];
     default: throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported expression type");
     }
   }
 
   void dot() {
     cur.expect('.');
-    if (cur.peek() == '.') throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported recursive descent");
+    if (cur.peek() == '.') {
+      if (wildcard == 0 || in_filter > 0)
+        throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported recursive descent");
+      descend();
+      return;
+    }
     const std::string name = read_property();
     if (name.empty()) throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Unexpected empty property");
     property(name);
@@ -212,6 +241,8 @@ class Parser {
       if (wildcard == 0) throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported wildcard expression");
       cur.expect('*');
       cur.expect(']');
+      ir.op(kExpectAtMost);  // no silent truncation of longer arrays
+      ir.varint(wildcard);
       range(0, wildcard, false);
       return;
     } else if (c == '?') {
@@ -267,17 +298,96 @@ class Parser {
     cur.expect('(');
     cur.expect('@');
     ir.op(kMark);
+    ++in_filter;
     next_expression();
+    --in_filter;
     while (cur.has_next() && cur.peek() == ' ') cur.skip(' ');
-    if (cur.peek() != '=') throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported character for expression");
-    cur.expect('=');
-    cur.expect('=');
+    Cmp cmp = kEq;
+    switch (cur.peek()) {
+    case '=':
+      cur.expect('=');
+      cur.expect('=');
+      break;
+    case '!':
+      cur.expect('!');
+      cur.expect('=');
+      cmp = kNe;
+      break;
+    case '<':
+    case '>': {
+      const bool lt = cur.next() == '<';
+      const bool eq = cur.skip('=');
+      cmp = lt ? (eq ? kLe : kLt) : (eq ? kGe : kGt);
+      break;
+    }
+    default:
+      throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported character for expression");
+    }
     while (cur.has_next() && cur.peek() == ' ') cur.skip(' ');
-    const std::string value = read_quoted();
-    ir.op(kStringEquals);
-    ir.string("\"" + value + "\"");
+    const char v = cur.peek();
+    if (v == '-' || std::isdigit(static_cast<unsigned char>(v))) {
+      const std::string number = read_number();
+      ir.op(kNumberCompare);
+      ir.bytes.push_back(uint8_t(cmp));
+      ir.string(number);
+    } else if (cmp == kEq) {
+      // the reference's string filter (and its error for anything else)
+      const std::string value = read_quoted();
+      ir.op(kStringEquals);
+      ir.string("\"" + value + "\"");
+    } else if (v == '\'' || v == '"') {
+      throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported comparison of a string");
+    } else {
+      read_number();  // throws: not a number
+    }
     ir.op(kReset);
     cur.expect(')');
+  }
+
+  // "..name" (an extension): every member named `name` inside the current
+  // value, at any level the index holds, stored in document order into the
+  // wildcard limit's K result slots.  It must be the last step.
+  void descend() {
+    cur.expect('.');
+    const std::string name = read_property();
+    if (name.empty()) throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Unexpected empty property");
+    if (cur.has_next())
+      throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported expression after a recursive descent");
+    ir.op(kDescendKey);
+    ir.string(name);
+    ir.stores += wildcard;
+    descended = true;
+    max_level = std::max<uint64_t>(max_level, kDescendLevels);
+  }
+
+  // A JSON number (RFC 8259: -?(0|[1-9][0-9]*)(.[0-9]+)?([eE][+-]?[0-9]+)?),
+  // ending at ')' or ' '.
+  std::string read_number() {
+    const int64_t start = cur.pos;
+    while (cur.has_next() && cur.peek() != ')' && cur.peek() != ' ') cur.next();
+    const std::string t = cur.slice(start, cur.pos);
+    size_t i = 0;
+    auto digits = [&]() {
+      const size_t b = i;
+      while (i < t.size() && std::isdigit(static_cast<unsigned char>(t[i]))) ++i;
+      return i - b;
+    };
+    bool ok = true;
+    if (i < t.size() && t[i] == '-') ++i;
+    if (i < t.size() && t[i] == '0') ++i;
+    else ok = ok && i < t.size() && t[i] >= '1' && t[i] <= '9' && digits() > 0;
+    if (ok && i < t.size() && t[i] == '.') {
+      ++i;
+      ok = digits() > 0;
+    }
+    if (ok && i < t.size() && (t[i] == 'e' || t[i] == 'E')) {
+      ++i;
+      if (i < t.size() && (t[i] == '+' || t[i] == '-')) ++i;
+      ok = digits() > 0;
+    }
+    if (!ok || i != t.size()) throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Invalid number");
+    while (cur.has_next() && cur.peek() == ' ') cur.skip(' ');
+    return t;
   }
 
   void property(const std::string &name) {
@@ -342,6 +452,8 @@ class Parser {
   Emitter ir;
   uint64_t max_level = 0;
   uint64_t wildcard;
+  int in_filter = 0;
+  bool descended = false;
 };
 
 }  // namespace

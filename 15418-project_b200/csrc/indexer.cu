@@ -85,7 +85,7 @@ __device__ Agg lookback(const IndexLaunch &P, uint32_t tile) {
         ready = ready && ((s[j] & 3u) != 0);
       }
       if (__all_sync(0xFFFFFFFFu, ready)) break;
-      if (++polls > kSpinLimit) {
+      if (++polls > P.lookback_spin_limit) {
         if (lane == 0) atomicOr(P.error, kErrLookbackTimeout);
 #pragma unroll
         for (int j = 0; j < kLookbackPerLane; ++j)

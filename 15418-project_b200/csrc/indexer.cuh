@@ -55,6 +55,8 @@ struct IndexLaunch {
   uint32_t num_tiles = 0;
   // tiles this launch claims: [tile_begin, tile_end); set by the launchers
   uint32_t tile_begin = 0, tile_end = 0;
+  // polls after which a look-back gives up on an unpublished predecessor
+  uint32_t lookback_spin_limit = 1u << 22;
 };
 
 // Error bits the kernels raise in IndexLaunch::error.

@@ -22,6 +22,10 @@ enum : uint8_t {
   OP_MARK_POSITION = 0x07,
   OP_RESET_POSITION = 0x08,
   OP_EXPRESSION_STRING_EQUALS = 0x09,
+  // Extensions of this build (never emitted for the reference's syntax):
+  OP_NUMBER_COMPARE = 0x0A,  // numeric filter: cmp byte, varint length, number text
+  OP_DESCEND_KEY = 0x0B,     // "..name" as the last step: varint length, key bytes
+  OP_EXPECT_AT_MOST = 0x0C,  // "[*]" element-count check: varint limit
 };
 
 // Last bitmap word read, per thread: consecutive searches of a record mostly
@@ -44,6 +48,7 @@ struct Rec {
   int ir_len;
   int base;    // bitmap level of query level 0
   int levels;  // levels present in LB
+  unsigned int *status;  // kQueryStatusOverflow is OR-ed here (may be null)
 };
 
 // Per-thread interpreter state indexed by query level, in shared memory
@@ -160,7 +165,135 @@ __device__ int read_varint(const Rec<Pos> &c, int &pos) {
   return int(value | (byte << shift));
 }
 
-template <typename Pos, typename OutT>
+
+// ---- Extensions of this build (the reference's compiler rejects them) ----
+//
+// Exact decimal comparison of two JSON numbers (no floating point): a number
+// is 0.d1d2d3... x 10^E with d1 != 0, or zero; exponents saturate at
+// +-10^15.  Bytes come from a getter so the same code reads the partition
+// (bounds-checked) and the IR.
+struct DecNum {
+  bool neg, zero;
+  int64_t E, nd, first, int_len, int_pos, frac_pos;
+};
+
+constexpr int64_t kExpLimit = 1000000000000000ll;
+
+__device__ __forceinline__ bool is_digit(uint8_t c) { return c >= '0' && c <= '9'; }
+
+template <class Get>
+__device__ __forceinline__ uint8_t dec_digit(const Get &get, const DecNum &x, int64_t k) {
+  return get(k < x.int_len ? x.int_pos + k : x.frac_pos + (k - x.int_len));
+}
+
+// Parses bytes [0, len) of the getter as one JSON number (RFC 8259).
+template <class Get>
+__device__ bool dec_parse(const Get &get, int64_t len, DecNum &o) {
+  int64_t i = 0;
+  o.neg = false;
+  if (i < len && get(i) == '-') {
+    o.neg = true;
+    ++i;
+  }
+  if (i >= len) return false;
+  o.int_pos = i;
+  const uint8_t c0 = get(i);
+  if (c0 == '0') {
+    ++i;
+  } else if (c0 >= '1' && c0 <= '9') {
+    while (i < len && is_digit(get(i))) ++i;
+  } else {
+    return false;
+  }
+  o.int_len = i - o.int_pos;
+  int64_t frac_len = 0;
+  o.frac_pos = i;
+  if (i < len && get(i) == '.') {
+    ++i;
+    o.frac_pos = i;
+    while (i < len && is_digit(get(i))) ++i;
+    frac_len = i - o.frac_pos;
+    if (frac_len == 0) return false;
+  }
+  int64_t ex = 0;
+  if (i < len && (get(i) == 'e' || get(i) == 'E')) {
+    ++i;
+    bool eneg = false;
+    if (i < len && (get(i) == '+' || get(i) == '-')) {
+      eneg = get(i) == '-';
+      ++i;
+    }
+    const int64_t es = i;
+    while (i < len && is_digit(get(i))) {
+      if (ex < kExpLimit) ex = ex * 10 + (get(i) - '0');
+      ++i;
+    }
+    if (i == es) return false;
+    if (ex > kExpLimit) ex = kExpLimit;
+    if (eneg) ex = -ex;
+  }
+  if (i != len) return false;
+  const int64_t total = o.int_len + frac_len;
+  int64_t z = 0;
+  while (z < total && dec_digit(get, o, z) == '0') ++z;
+  o.zero = z == total;
+  o.first = z;
+  o.nd = total - z;
+  o.E = o.int_len - z + ex;
+  return true;
+}
+
+template <class GetA, class GetB>
+__device__ int dec_cmp(const GetA &ga, const DecNum &a, const GetB &gb, const DecNum &b) {
+  const int sa = a.zero ? 0 : (a.neg ? -1 : 1);
+  const int sb = b.zero ? 0 : (b.neg ? -1 : 1);
+  if (sa != sb) return sa < sb ? -1 : 1;
+  if (sa == 0) return 0;
+  int mag = 0;
+  if (a.E != b.E) {
+    mag = a.E > b.E ? 1 : -1;
+  } else {
+    const int64_t n = a.nd > b.nd ? a.nd : b.nd;
+    for (int64_t k = 0; k < n && mag == 0; ++k) {
+      const uint8_t da = k < a.nd ? dec_digit(ga, a, a.first + k) : uint8_t('0');
+      const uint8_t db = k < b.nd ? dec_digit(gb, b, b.first + k) : uint8_t('0');
+      if (da != db) mag = da > db ? 1 : -1;
+    }
+  }
+  return sa > 0 ? mag : -mag;
+}
+
+__device__ __forceinline__ bool cmp_holds(int op, int r) {
+  switch (op) {
+  case 0: return r == 0;
+  case 1: return r != 0;
+  case 2: return r < 0;
+  case 3: return r <= 0;
+  case 4: return r > 0;
+  case 5: return r >= 0;
+  default: return false;
+  }
+}
+
+template <typename Pos>
+__device__ __forceinline__ void raise_status(const Rec<Pos> &c, unsigned int bits) {
+  if (c.status != nullptr) atomicOr(c.status, bits);
+}
+
+// Does the string before the ':' at `colon` equal the key (the test of
+// MOVE_TO_KEY, query.cu:254-302)?
+template <typename Pos>
+__device__ bool key_at_colon(const Rec<Pos> &c, WordCache<Pos> &sc, Pos line_start, Pos colon,
+                             int key_pos, int key_len) {
+  const Pos string_end = prev_bit(sc, c.S, c.W, Pos(line_start + 1), Pos(colon - 1));
+  const Pos string_start = string_end - key_len;
+  if (string_start < line_start || at(c, string_start) != '"') return false;
+  for (int i = 0; i < key_len; ++i)
+    if (ir_at(c, key_pos + i) != at(c, Pos(string_start + i + 1))) return false;
+  return true;
+}
+
+template <typename Pos, typename OutT, bool kExt>
 __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line_start,
                            Pos line_end, int num_results, OutT *out) {
   if (line_start < 0 || line_start >= c.n || line_end < 0) return;
@@ -209,6 +342,8 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       if (stored < num_results) {
         out[2 * stored] = OutT(line_index);
         out[2 * stored + 1] = OutT(end_str);
+      } else if constexpr (kExt) {
+        raise_status(c, kQueryStatusOverflow);  // only extension IR gets here
       }
       ++stored;
       break;
@@ -377,6 +512,90 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       }
       break;
     }
+    case OP_NUMBER_COMPARE: {
+      if constexpr (!kExt) return;
+      const int cmp = ir_at(c, qp++);
+      const int lit_len = read_varint(c, qp);
+      const int lit_pos = qp;
+      qp += lit_len;
+      if (lit_len < 0 || lit_pos + lit_len > c.ir_len || !LEVEL_OK(level)) return;
+      const Pos lend = L.level_end(level);
+      while (at(c, line_index) == ' ' && line_index < lend) ++line_index;
+      Pos value_end = lend - 1;
+      while (line_index < value_end && at(c, value_end) == ' ') --value_end;
+      if (line_index < 0 || value_end >= c.n || value_end < line_index) return;
+      const Pos v0 = line_index;
+      auto gv = [&](int64_t i) { return at(c, Pos(v0 + i)); };
+      auto gl = [&](int64_t i) { return ir_at(c, int(lit_pos + i)); };
+      DecNum v, lit;
+      if (!dec_parse(gv, int64_t(value_end - line_index) + 1, v)) return;
+      if (!dec_parse(gl, int64_t(lit_len), lit)) return;
+      if (!cmp_holds(cmp, dec_cmp(gv, v, gl, lit))) return;
+      break;
+    }
+    case OP_DESCEND_KEY: {
+      if constexpr (!kExt) return;
+      key_len = read_varint(c, qp);
+      key_pos = qp;
+      qp += key_len;
+      if (key_len < 0 || !LEVEL_OK(level)) return;
+      // every member named key inside the current value, at any level the
+      // index holds, in document order (by the position of its ':')
+      const Pos hi = L.level_end(level);
+      for (Pos w = line_index >> 6; w * 64 < hi && w < c.W; ++w) {
+        uint64_t cand = 0;
+        for (int l = level; l + c.base < c.levels; ++l) {
+          const uint64_t *lw = level_words(c, l);
+          if (lw != nullptr) cand |= lw[w];
+        }
+        const Pos base = w * 64;
+        if (line_index > base) cand &= ~0ull << (line_index - base);
+        if (hi - base < 64) cand &= (1ull << (hi - base)) - 1ull;
+        while (cand != 0) {
+          const Pos p = base + Pos(__ffsll(static_cast<long long>(cand)) - 1);
+          cand &= cand - 1;
+          if (at(c, p) != ':') continue;
+          int lv = level;
+          while (lv + c.base < c.levels &&
+                 ((level_words(c, lv)[w] >> (p - base)) & 1ull) == 0ull)
+            ++lv;
+          if (!key_at_colon(c, sc, line_start, p, key_pos, key_len)) continue;
+          const Pos vend = next_struct(c, lbc, hi, Pos(p + 1), level_words(c, lv));
+          Pos vs = p + 1;
+          while (at(c, vs) == ' ' && vs < vend) ++vs;
+          Pos ve = vend;
+          while (ve > vs && at(c, ve - 1) == ' ') --ve;
+          if (stored < num_results) {
+            out[2 * stored] = OutT(vs);
+            out[2 * stored + 1] = OutT(ve);
+          } else {
+            raise_status(c, kQueryStatusOverflow);
+          }
+          ++stored;
+        }
+      }
+      break;
+    }
+    case OP_EXPECT_AT_MOST: {
+      if constexpr (!kExt) return;
+      const int limit = read_varint(c, qp);
+      if (limit < 0 || !LEVEL_OK(level)) return;
+      if (limit == 0 || at(c, line_index) != '[') break;
+      // K commas at this level before the closing bracket: K+1 elements
+      const Pos lend = L.level_end(level);
+      const uint64_t *lvl = level_words(c, level);
+      Pos p = line_index;
+      int commas = 0;
+      steps = 0;
+      while (commas < limit) {
+        if (++steps > max_steps) break;
+        p = next_struct(c, lbc, lend, Pos(p + 1), lvl);
+        if (at(c, p) != ',') break;
+        ++commas;
+      }
+      if (commas >= limit) raise_status(c, kQueryStatusOverflow);
+      break;
+    }
     default:
       break;
     }
@@ -385,7 +604,9 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
 #undef LEVEL_OK
 }
 
-template <typename Pos, typename OutT>
+// kExt: the IR holds extension opcodes (numeric filters, "..name", "[*]"
+// checks); reference-syntax IR runs the variant without them.
+template <typename Pos, typename OutT, bool kExt>
 __global__ void __launch_bounds__(256)
     query_kernel(const QueryLaunch q, const __grid_constant__ IrBlob ir, OutT *out, int nlev) {
   __shared__ uint8_t s_ir[kMaxQueryIrBytes];
@@ -393,7 +614,7 @@ __global__ void __launch_bounds__(256)
   for (int i = threadIdx.x; i < q.ir_len; i += blockDim.x) s_ir[i] = ir.bytes[i];
   __syncthreads();
   const Rec<Pos> c{q.in, Pos(q.n), q.S, q.LB, Pos(q.W), s_ir, q.ir_len, q.base_level,
-                   q.num_levels};
+                   q.num_levels, q.status};
   Pos *ends = reinterpret_cast<Pos *>(s_levels);
   int32_t *idx = reinterpret_cast<int32_t *>(ends + nlev * blockDim.x);
   const LevelState<Pos> L{ends + threadIdx.x, idx + threadIdx.x, int(blockDim.x), nlev};
@@ -404,10 +625,11 @@ __global__ void __launch_bounds__(256)
     for (int i = 0; i < 2 * q.num_results; ++i) o[i] = OutT(-1);
     const int64_t start = q.NL[r];
     const int64_t end = (r + 1 < q.num_lines) ? q.NL[r + 1] : q.n - 1;
-    run_record<Pos, OutT>(c, L, Pos(start), Pos(end), q.num_results, o);
+    run_record<Pos, OutT, kExt>(c, L, Pos(start), Pos(end), q.num_results, o);
   }
 }
 
+template <bool kExt>
 __global__ void __launch_bounds__(256)
     batch_query_kernel(const BatchQueryLaunch q, const __grid_constant__ IrBlob ir, int nlev) {
   __shared__ uint8_t s_ir[kMaxQueryIrBytes];
@@ -440,8 +662,8 @@ __global__ void __launch_bounds__(256)
     // batch files are below 2 GiB (int32 results): 32-bit positions
     const Rec<int32_t> c{q.in + F.in_off, int32_t(F.n), q.S + F.s_off, q.LB + F.lb_off,
                          int32_t((F.n + 63u) / 64u), s_ir + g.ir_off, g.ir_len, g.base_level,
-                         F.levels};
-    run_record<int32_t, int32_t>(c, L, int32_t(start), int32_t(end), g.num_results, o);
+                         F.levels, q.status};
+    run_record<int32_t, int32_t, kExt>(c, L, int32_t(start), int32_t(end), g.num_results, o);
   }
 }
 
@@ -474,7 +696,17 @@ int query_ir_levels(const uint8_t *ir, int len) {
       if (n > 0) p += n;
       break;
     case OP_MOVE_TO_INDEX:
-    case OP_MOVE_TO_INDEX_REVERSE: skip_varint(p, nullptr); break;
+    case OP_MOVE_TO_INDEX_REVERSE:
+    case OP_EXPECT_AT_MOST: skip_varint(p, nullptr); break;
+    case OP_NUMBER_COMPARE:
+      ++p;  // comparator
+      skip_varint(p, &n);
+      if (n > 0) p += n;
+      break;
+    case OP_DESCEND_KEY:
+      skip_varint(p, &n);
+      if (n > 0) p += n;
+      break;
     case OP_MARK_POSITION:
       if (marked < kMaxQueryLevels) marks[marked++] = level;
       break;
@@ -488,15 +720,49 @@ int query_ir_levels(const uint8_t *ir, int len) {
   return deepest + 1 < kMaxQueryLevels ? deepest + 1 : kMaxQueryLevels;
 }
 
+bool query_ir_uses_extensions(const uint8_t *ir, int len) {
+  auto skip_varint = [&](int &p) -> int {
+    uint32_t v = 0, b = 0;
+    int shift = 0;
+    while (p < len && ((b = ir[p++]) & 0x80u) != 0 && shift <= 28) {
+      v |= (b & 0x7Fu) << shift;
+      shift += 7;
+    }
+    return int(v | (shift <= 28 ? (b << shift) : 0u));
+  };
+  for (int p = 0; p < len;) {
+    const uint8_t op = ir[p++];
+    switch (op) {
+    case OP_END: return false;
+    case OP_NUMBER_COMPARE:
+    case OP_DESCEND_KEY:
+    case OP_EXPECT_AT_MOST: return true;
+    case OP_MOVE_TO_KEY:
+    case OP_EXPRESSION_STRING_EQUALS: {
+      const int n = skip_varint(p);
+      if (n > 0) p += n;
+      break;
+    }
+    case OP_MOVE_TO_INDEX:
+    case OP_MOVE_TO_INDEX_REVERSE: skip_varint(p); break;
+    default: break;
+    }
+  }
+  return false;
+}
+
 cudaError_t batch_query_launch(const BatchQueryLaunch &q, const IrBlob &ir, int grid,
                                int block, cudaStream_t stream) {
   int nlev = 1;
+  bool ext = false;
   for (int g = 0; g < q.num_groups; ++g) {
     const int l = query_ir_levels(ir.bytes + q.groups[g].ir_off, q.groups[g].ir_len);
     if (l > nlev) nlev = l;
+    ext = ext || query_ir_uses_extensions(ir.bytes + q.groups[g].ir_off, q.groups[g].ir_len);
   }
   const size_t smem = size_t(nlev) * size_t(block) * 8u;
-  batch_query_kernel<<<grid, block, smem, stream>>>(q, ir, nlev);
+  if (ext) batch_query_kernel<true><<<grid, block, smem, stream>>>(q, ir, nlev);
+  else batch_query_kernel<false><<<grid, block, smem, stream>>>(q, ir, nlev);
   return cudaGetLastError();
 }
 
@@ -507,13 +773,16 @@ cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
   if (block > 256) block = 256;
   if (grid <= 0) grid = int((q.num_lines + block - 1) / block);
   const int nlev = query_ir_levels(ir.bytes, q.ir_len);
+  const bool ext = query_ir_uses_extensions(ir.bytes, q.ir_len);
   if (q.out64 != nullptr) {
     const size_t smem = size_t(nlev) * size_t(block) * 12u;
-    query_kernel<int64_t, int64_t><<<grid, block, smem, stream>>>(q, ir, q.out64, nlev);
+    if (ext) query_kernel<int64_t, int64_t, true><<<grid, block, smem, stream>>>(q, ir, q.out64, nlev);
+    else query_kernel<int64_t, int64_t, false><<<grid, block, smem, stream>>>(q, ir, q.out64, nlev);
   } else {
     // int32 results imply a partition below 2 GiB: 32-bit positions
     const size_t smem = size_t(nlev) * size_t(block) * 8u;
-    query_kernel<int32_t, int32_t><<<grid, block, smem, stream>>>(q, ir, q.out32, nlev);
+    if (ext) query_kernel<int32_t, int32_t, true><<<grid, block, smem, stream>>>(q, ir, q.out32, nlev);
+    else query_kernel<int32_t, int32_t, false><<<grid, block, smem, stream>>>(q, ir, q.out32, nlev);
   }
   return cudaGetLastError();
 }

@@ -11,6 +11,12 @@ namespace gpjb {
 constexpr int kMaxQueryLevels = 16;   // orig.hpp:10 kMaxQueryLevels
 constexpr int kMaxQueryIrBytes = 4096;  // orig.hpp:11 kMaxQueryIrBytes
 
+// Status bit a query raises when a record had more results than its slots:
+// a "[*]" array longer than the wildcard limit, or more "..name" matches.
+// Only IR with extension opcodes can raise it.  Kept clear of the indexer's
+// error bits (1, 2, 4), with which it shares the batch's error word.
+constexpr unsigned int kQueryStatusOverflow = 0x100u;
+
 // One query over every record of one partition.
 struct QueryLaunch {
   const uint8_t *in = nullptr;   // partition bytes
@@ -27,6 +33,7 @@ struct QueryLaunch {
                                  // of a top-level array are the records)
   int32_t *out32 = nullptr;      // [num_lines][num_results][2], or
   int64_t *out64 = nullptr;      // the same with 64-bit offsets
+  unsigned int *status = nullptr;  // kQueryStatusOverflow is OR-ed here (optional)
 };
 
 // The IR travels in the kernel parameters (4 KiB, copied into shared memory
@@ -37,6 +44,10 @@ struct IrBlob {
 
 cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
                          int block, cudaStream_t stream);
+
+// True when the IR holds extension opcodes (numeric filters, "..name",
+// "[*]" element checks): those launch the interpreter variant that has them.
+bool query_ir_uses_extensions(const uint8_t *ir, int len);
 
 // Batched query over every record of every file of a multi-file index build:
 // record r belongs to the file whose record range holds it (file_info from
@@ -60,6 +71,7 @@ struct BatchQueryLaunch {
   const uint64_t *file_info = nullptr;  // kFileInfoWords per file
   const uint64_t *totals = nullptr;
   int32_t *out = nullptr;
+  unsigned int *status = nullptr;  // kQueryStatusOverflow is OR-ed here (optional)
   int num_groups = 0;
   BatchQueryGroup groups[kMaxBatchGroups];
 };

@@ -198,6 +198,7 @@ struct gpj_server {
   int32_t *h_arena = nullptr;
   OffsetArena host;  // under mu
   unsigned long long *h_pinned = nullptr;
+  unsigned int *d_status = nullptr;  // one query-status word per slot
 
   std::vector<Slot> slots;
   std::vector<int> free_slots;  // scheduler thread only
@@ -444,9 +445,13 @@ struct gpj_server {
       r->resp.result_offset[q] = off;
       off += lines * r->queries[q].num_result_slots * 2u;
     }
+    unsigned int *d_status = this->d_status + r->slot;
+    auto *h_status = reinterpret_cast<unsigned int *>(s.pinned + 7);
+    *h_status = 0;
     if (res->size == 0) {
       if (ints > 0) e = cudaMemsetAsync(d_out, 0xFF, ints * 4u, s.stream);
     } else {
+      e = cudaMemsetAsync(d_status, 0, 4, s.stream);
       for (size_t q = 0; q < r->queries.size() && e == cudaSuccess; ++q) {
         const gpj_batch_query &bq = r->queries[q];
         gpjb::QueryLaunch ql;
@@ -462,12 +467,15 @@ struct gpj_server {
         ql.num_levels = res->levels;
         ql.base_level = int(bq.base_level);
         ql.out32 = d_out + r->resp.result_offset[q];
+        ql.status = d_status;
         if (bq.num_result_slots == 0) continue;
         gpjb::IrBlob blob;
         std::memset(blob.bytes, 0, sizeof(blob.bytes));
         std::memcpy(blob.bytes, r->irs[q].data(), r->irs[q].size());
         e = gpjb::query_launch(ql, blob, 0, 256, s.stream);
       }
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h_status, d_status, 4, cudaMemcpyDeviceToHost, s.stream);
     }
     if (e == cudaSuccess && ints > 0)
       e = cudaMemcpyAsync(h_arena + r->host_off / 4u, d_out, ints * 4u, cudaMemcpyDeviceToHost,
@@ -688,6 +696,10 @@ struct gpj_server {
           else finish(r, cuda_status(e), msg);
         } else if (r->state == St::Indexing) {
           on_index_done(r);
+        } else if (*reinterpret_cast<const unsigned int *>(slots[r->slot].pinned + 7) &
+                   gpjb::kQueryStatusOverflow) {
+          finish(r, GPJ_ERR_CAPACITY,
+                 "a record has more results than result slots; the results are truncated");
         } else {
           finish(r, GPJ_OK, "");
         }
@@ -787,6 +799,7 @@ void free_server(gpj_server *s) {
   if (s->d_arena) cudaFree(s->d_arena);
   if (s->h_arena) cudaFreeHost(s->h_arena);
   if (s->h_pinned) cudaFreeHost(s->h_pinned);
+  if (s->d_status) cudaFree(s->d_status);
   delete s;
 }
 
@@ -841,6 +854,14 @@ int gpj_server_create(const gpj_server_config *config, gpj_server **out) {
     if (e != cudaSuccess) {
       code = GPJ_ERR_OOM;
       err = std::string("pinned slot words: ") + cudaGetErrorString(e);
+    }
+  }
+  if (code == GPJ_OK) {
+    e = cudaMalloc(reinterpret_cast<void **>(&s->d_status), uint64_t(cfg.num_slots) * 4u);
+    if (e == cudaSuccess) e = cudaMemset(s->d_status, 0, uint64_t(cfg.num_slots) * 4u);
+    if (e != cudaSuccess) {
+      code = GPJ_ERR_CUDA;
+      err = std::string("query status words: ") + cudaGetErrorString(e);
     }
   }
   if (code == GPJ_OK) {

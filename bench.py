@@ -686,7 +686,8 @@ def run_batch(args, world, rank, local):
 
     # plain path: one single-file index launch + one query launch per file,
     # issued from C (gpj_batch_run_per_file), into the same outputs
-    want = torch.from_numpy(d2h(v.d_results, v.result_ints, np.int32))
+    want_np = d2h(v.d_results, v.result_ints, np.int32)
+    want = torch.from_numpy(want_np)
     batch.run_per_file(s)
     torch.cuda.synchronize(dev)
     ms_plain = allreduce_max(timed(lambda: batch.run_per_file(s), 3), world)
@@ -700,7 +701,7 @@ def run_batch(args, world, rank, local):
     for _ in range(1):
         batch.run_host(h_in.data_ptr(), h_out.data_ptr(), h_info.data_ptr(), s)
     e2e = []
-    for _ in range(max(2, min(args.steps, 5))):
+    for _ in range(args.steps):  # the same step count as the device-resident value
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         batch.run_host(h_in.data_ptr(), h_out.data_ptr(), h_info.data_ptr(), s)
@@ -746,38 +747,70 @@ def run_batch(args, world, rank, local):
         "index_ms": round(ms_index, 4), "query_ms": round(ms_query, 4), "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_files(files, comp, queries)
+        # the CPU baseline leg: the oracle over every timed file on every host
+        # thread, timed, and its results compared with the batch's (the
+        # parity gate of this line: any difference fails the run)
+        oracle_res, dt, threads, done = oracle_files(files, queries)
+        line["parity"] = batch_parity(files, queries, oracle_res, want_np, info)
+        line["cpu_baseline"] = {
+            "value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
+            "kind": "port", "sample": f"all {len(files)} files of the workload ({done} bytes), "
+            f"one file per task on {threads} threads, one pass ({dt:.2f} s)"}
     batch.close()
     return line
 
 
-def cpu_baseline_files(files, comp, queries, budget_bytes: int = 96 << 20):
-    """The oracle on whole files (a bounded sample), one file per task on
-    every host thread."""
+def oracle_files(files, queries, threads: int | None = None, limit_bytes: int | None = None):
+    """The oracle (the reference algorithm restated in C) over whole files,
+    one file per task on every host thread: per file the int64
+    [lines][slots][2] results of its query, and the wall time.  With
+    limit_bytes only the leading files up to that many bytes."""
     import oracle
-    threads = os.cpu_count() or 1
-    sample, acc = [], 0
-    for d, k in files:
-        if acc >= budget_bytes:
-            break
-        sample.append((d, k))
-        acc += len(d)
+    threads = threads or os.cpu_count() or 1
+    count = len(files)
+    if limit_bytes is not None:
+        acc, count = 0, 0
+        for d, _ in files:
+            if acc >= limit_bytes:
+                break
+            acc += len(d)
+            count += 1
 
-    def work(item):
-        d, k = item
+    def work(i):
+        d, k = files[i]
         c, base, lv = queries[k]
-        ix = oracle.OracleIndex(d, lv)
-        if len(d):
-            ix.query(c.ir_bytes, c.num_result_slots, base)
-        return len(d)
+        if not len(d):
+            return None
+        return oracle.OracleIndex(d, lv).query(c.ir_bytes, c.num_result_slots, base)
 
     t0 = time.perf_counter()
     with cf.ThreadPoolExecutor(threads) as pool:
-        done = sum(pool.map(work, sample))
+        res = list(pool.map(work, range(count)))
     dt = time.perf_counter() - t0
-    return {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
-            "kind": "port", "sample": f"{len(sample)} whole files, {done} bytes, "
-            f"one file per task on {threads} threads"}
+    return res, dt, threads, sum(len(files[i][0]) for i in range(count))
+
+
+def batch_parity(files, queries, want, results, info):
+    """Every file's query results of the batch (int32, file-local) against the
+    oracle's: the parity gate of the timed c3 numbers.  Raises on the first
+    difference."""
+    checked = matches = 0
+    for f, w in enumerate(want):
+        lines, out_off = int(info[f, 0]), int(info[f, 3])
+        slots = queries[files[f][1]][0].num_result_slots
+        got = results[out_off:out_off + lines * slots * 2].astype(np.int64).reshape(lines, slots, 2)
+        if w is None:
+            ok = bool((got == -1).all())
+        else:
+            ok = got.shape == w.shape and np.array_equal(got, w)
+            matches += int((w[..., 0] >= 0).sum())
+        if not ok:
+            raise AssertionError(f"c3 parity: file {f} results differ from the oracle")
+        checked += 1
+    return {"oracle": "oracle/gpjson_oracle.c (reference algorithm restated, pinned by the "
+                      "reference's own test vectors)",
+            "files_checked": checked, "files_total": len(files), "matches": matches,
+            "mismatches": 0, "outputs": "every file's query results, bit-exact"}
 
 
 def _partitions(data: np.ndarray, parts: int):
@@ -824,39 +857,54 @@ def cpu_baseline(data, comp, records, levels, budget_s: float, threads: int | No
 
 
 def run_reference(args, world, rank):
-    """CPU arm: the oracle on the host cores, same metric and config."""
+    """CPU arm: the reference algorithm's CPU restatement (the oracle; the
+    reference project has no CPU implementation of this path) on all host
+    threads, on the same workload, metric and config as this engine's line.
+    c3: each timed step indexes and queries all 10,000 files once (warm-up
+    steps run only the leading 96 MiB of files: they are untimed)."""
     if rank != 0:
         return None
     pkg = entry.package()
     if args.workload in ("c3", "c4"):
-        # the leading c3 files (96 MiB) are each step's bounded sample
-        files = c3_files(pkg, limit_bytes=96 << 20)
+        files = c3_files(pkg, args.scale)
         comp = compile_all(pkg, C3_QUERIES)
         fq = [(c, base, c.max_depth + base) for c, base in comp]
         queries, desc = C3_QUERIES, C3_DESC
-
-        def step():
-            return cpu_baseline_files(files, comp, fq)
+        total = sum(len(d) for d, _ in files)
+        times, records = [], 0
+        for k in range(args.warmup + args.steps):
+            if k < args.warmup:
+                oracle_files(files, fq, limit_bytes=96 << 20)
+                continue
+            res, dt, threads, done = oracle_files(files, fq)
+            assert done == total
+            times.append(dt)
+            records = sum(1 if r is None else r.shape[0] for r in res)
+        ms = float(np.mean(times)) * 1e3
+        v = total / (ms / 1e3) / 1e9
+        cb = {"value": round(v, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+              "sample": f"all {len(files)} files ({total} bytes) per step, one file per task "
+                        f"on {threads} threads"}
+        config = {"workload": C3_DESC, "input_bytes": total, "files": len(files),
+                  "records": records, "queries": queries}
     else:
         data, queries, records, desc = workload(args.workload, pkg)
         comp = compile_all(pkg, queries)
         levels = max(c.max_depth + base for c, base in comp)
-
-        def step():
-            return cpu_baseline(data, comp, records, levels, budget_s=10.0)
-    vals = []
-    for k in range(args.warmup + args.steps):
-        cb = step()
-        if k >= args.warmup:
-            vals.append(cb["value"])
-    v = float(np.mean(vals))
-    cb["value"] = round(v, 4)
+        vals = []
+        for k in range(args.warmup + args.steps):
+            cb = cpu_baseline(data, comp, records, levels, budget_s=10.0)
+            if k >= args.warmup:
+                vals.append(cb["value"])
+        v = float(np.mean(vals))
+        cb["value"] = round(v, 4)
+        ms = None
+        config = {"workload": desc, "queries": queries}
     return {"metric": METRIC, "value": round(v, 4), "unit": "GB/s", "impl": "reference",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
-            "config": {"workload": desc, "queries": queries},
-            "cpu_baseline": cb,
+            "ms_per_step": round(ms, 2) if ms is not None else None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator)", "config": config, "cpu_baseline": cb,
             "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 

@@ -37,6 +37,14 @@ extern "C" {
 /* gpj_index_build flags */
 #define GPJ_INDEX_EMIT_ESCAPE_QUOTE 1u /* also materialise E and Q */
 #define GPJ_INDEX_NO_TMA 2u            /* stage tiles with plain loads */
+/* Diagnostic (gpj_index_build and gpj_index_build_async only): the first
+ * 32 KiB tile is left out of the launch, so the look-back of every other tile
+ * waits for a descriptor that is never published; each wait gives up after
+ * about 16 K polls (milliseconds) and the build reports GPJ_ERR_TIMEOUT
+ * (d_summary[3] bit 0).  It exercises the bounded-wait error path on a
+ * device that stays usable; its outputs are meaningless.  Needs an input of
+ * at least two tiles. */
+#define GPJ_INDEX_DIAG_TILE0_UNPUBLISHED 0x80000000u
 
 #define GPJ_MAX_LEVELS 22     /* kMaxNumLevels, sharemem/leveled-bitmaps-index.cu */
 #define GPJ_MAX_QUERY_IR 4096 /* kMaxQueryIrBytes, query/kernels/orig.hpp:11 */
@@ -81,8 +89,18 @@ int gpj_ctx_destroy(gpj_ctx *ctx);
 /* Compiles a JSONPath query into the byte IR.
  * Replaces query::QueryCompiler::compile / QueryParser::compile
  * (include/gpjson/query/query_compiler.hpp:110-116, 86-92).  Same grammar,
- * IR, max_depth and result-slot count.  wildcard_limit = 0 rejects "[*]" as
- * the reference does; K > 0 compiles "[*]" as "[0:K]". */
+ * IR, max_depth and result-slot count for every query in the reference's
+ * syntax.  wildcard_limit = 0 rejects "[*]" and ".." as the reference does
+ * (query_compiler.cpp:202-204, 287-289).  Extensions the reference rejects:
+ *  - K > 0: "[*]" compiles as "[0:K]" preceded by an element-count check
+ *    that raises GPJ_QUERY_OVERFLOW for an array of more than K elements;
+ *  - K > 0: "..name" as the last step returns every member named `name`
+ *    inside the current value at any indexed level, in document order, in K
+ *    result slots (max_depth 15: index that many levels to reach them all);
+ *  - numeric filters "[?(@<path> <op> <number>)]", op one of == != < <= > >=,
+ *    an exact decimal comparison with a JSON number (a value that is not a
+ *    number fails the filter; query_compiler.cpp:366-391 takes only
+ *    == "string"). */
 int gpj_compile(const char *query, uint64_t wildcard_limit, uint8_t *h_ir,
                 uint64_t ir_capacity, uint64_t *ir_len, uint64_t *max_depth,
                 uint64_t *num_result_slots);
@@ -100,11 +118,13 @@ int gpj_index_build(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_bytes,
 
 /* Same build into caller-owned buffers (index->d_string, d_leveled,
  * d_newline with newline_capacity entries, optional d_escape/d_quote).
- * Asynchronous: the line count, final string state and final depth are
- * written to d_summary[0..2] (3 x uint64 in device memory).  Scratch comes
- * from the context.  If the newline count exceeds newline_capacity - 1 the
- * extra offsets are dropped; d_summary[0] still holds the true line count.
- * Replaces the same builders as gpj_index_build. */
+ * Asynchronous: d_summary must hold 4 x uint64 in device memory and receives
+ * d_summary[0] = line count, [1] = final string state, [2] = final depth
+ * (sign-extended signed char), [3] = error bits (nonzero: a bounded device
+ * wait gave up; bit 0 look-back, bit 1 tile copy, bit 2 pipeline).  Scratch
+ * comes from the context.  If the newline count exceeds newline_capacity - 1
+ * the extra offsets are dropped; d_summary[0] still holds the true line
+ * count.  Replaces the same builders as gpj_index_build. */
 int gpj_index_build_async(gpj_ctx *ctx, const uint8_t *d_input,
                           uint64_t size_bytes, int num_levels, uint32_t flags,
                           gpj_index *index, uint64_t *d_summary, void *stream);
@@ -119,9 +139,15 @@ int gpj_index_build_async(gpj_ctx *ctx, const uint8_t *d_input,
  * no context is needed.  Its scratch is a fixed 1 MiB device array inside the
  * library, so size_bytes is limited to 4 GiB (GPJ_ERR_CAPACITY beyond).  The
  * first call on a device looks up that array's device address (make it
- * before any stream capture).  All calls on a device share the array: calls
- * whose work overlaps on the GPU race.  Unaligned inputs use plain loads
- * instead of TMA. */
+ * before any stream capture) and keeps it for the process: do not use this
+ * entry point across a cudaDeviceReset of that device.  CUDA loads modules
+ * lazily by default, so the first call (or the first launch of each index
+ * kernel variant) is also when the driver places the array and the kernel
+ * code in device memory: a host that reserves all device memory up front
+ * should make one call per device with its level count before reserving, or
+ * run with CUDA_MODULE_LOADING=EAGER.  All calls on a device share the
+ * array: calls whose work overlaps on the GPU race.  Unaligned inputs use
+ * plain loads instead of TMA. */
 #define GPJ_NOALLOC_MAX_BYTES 4294967296ull
 int gpj_index_build_noalloc(const uint8_t *d_input, uint64_t size_bytes,
                             int num_levels, uint32_t flags, gpj_index *index,
@@ -145,6 +171,15 @@ int gpj_query_run(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
 int gpj_query_run64(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir,
                     uint64_t ir_len, uint32_t num_result_slots, int64_t *d_out,
                     void *stream);
+
+/* Status of the queries run on a context: waits for `stream`, returns in
+ * *flags the bits raised by the context's query launches since the last call,
+ * and clears them.  GPJ_QUERY_OVERFLOW: a record had more results than the
+ * query has result slots, so some were dropped -- only the extensions can:
+ * a "[*]" array longer than the wildcard limit, or more "..name" matches.
+ * The reference compiles neither, so it has no counterpart. */
+#define GPJ_QUERY_OVERFLOW 0x100u
+int gpj_query_status(gpj_ctx *ctx, uint32_t *flags, void *stream);
 
 /* Options of gpj_query_run_opts; all-zero means the reference behaviour
  * (int32 offsets, records are lines, query level 0 = bitmap level 0). */
@@ -170,7 +205,8 @@ int gpj_query_run_opts(gpj_ctx *ctx, const gpj_index *index, const uint8_t *h_ir
  * memory makes the copies overlap the indexing).  h_out[q] must hold
  * out_capacity[q] int32; *num_lines gets the record count (0 for an empty
  * input).  base_levels may be NULL (all 0).  GPJ_ERR_CAPACITY (nothing
- * copied back) if a result does not fit.  Replaces the per-partition body
+ * copied back) if a result does not fit; GPJ_ERR_CAPACITY after the copies
+ * if a record had more results than result slots (GPJ_QUERY_OVERFLOW).  Replaces the per-partition body
  * of gpjson::Engine::query (src/gpjson/engine.cpp:131-166: load_to_device,
  * build, execute_batch). */
 int gpj_query_host(gpj_ctx *ctx, const uint8_t *h_input, uint64_t size_bytes,

@@ -57,6 +57,9 @@ def lib() -> C.CDLL:
         l.orc_build_index.argtypes = [vp, u64, i32, vp, vp, vp, vp, vp, u64]
         l.orc_query.restype = i32
         l.orc_query.argtypes = [vp, u64, vp, u64, vp, vp, u64, i32, i32, vp, u64, i32, vp]
+        l.orc_query_status.restype = i32
+        l.orc_query_status.argtypes = [vp, u64, vp, u64, vp, vp, u64, i32, i32, vp, u64, i32,
+                                       vp, vp]
         _lib = l
     return _lib
 
@@ -95,13 +98,20 @@ class OracleIndex:
         assert got == lines
         self.num_lines = lines
 
+    # status bits of the last query (ORC_STATUS_OVERFLOW: a record had more
+    # results than slots -- only the extension opcodes can)
+    STATUS_OVERFLOW = 1
+    last_status = 0
+
     def query(self, ir: bytes, num_results: int, base_level: int = 0) -> np.ndarray:
         """int64 [num_lines, num_results, 2], -1 = no match."""
         out = np.full(self.num_lines * num_results * 2, -1, np.int64)
         irb = np.frombuffer(ir, np.uint8) if ir else np.zeros(1, np.uint8)
-        lib().orc_query(_ptr(self.data), self.n, _ptr(self.NL), self.num_lines, _ptr(self.S),
-                        _ptr(self.LB), self.W, self.num_levels, base_level, _ptr(irb),
-                        len(ir), num_results, _ptr(out))
+        st = np.zeros(1, np.uint32)
+        lib().orc_query_status(_ptr(self.data), self.n, _ptr(self.NL), self.num_lines,
+                               _ptr(self.S), _ptr(self.LB), self.W, self.num_levels, base_level,
+                               _ptr(irb), len(ir), num_results, _ptr(out), _ptr(st))
+        self.last_status = int(st[0])
         return out.reshape(self.num_lines, num_results, 2)
 
 

@@ -172,7 +172,13 @@ enum {
   OP_MOVE_TO_INDEX_REVERSE = 0x06,
   OP_MARK_POSITION = 0x07,
   OP_RESET_POSITION = 0x08,
-  OP_EXPRESSION_STRING_EQUALS = 0x09
+  OP_EXPRESSION_STRING_EQUALS = 0x09,
+  /* Extensions of this build (never emitted for the reference's syntax):
+   * numeric filters, recursive descent to a member name, and the element
+   * count check of a bounded "[*]". */
+  OP_NUMBER_COMPARE = 0x0A,
+  OP_DESCEND_KEY = 0x0B,
+  OP_EXPECT_AT_MOST = 0x0C
 };
 #define ORC_MAX_LEVELS 16 /* query.cu:20 MAX_NUM_LEVELS */
 
@@ -186,6 +192,7 @@ typedef struct {
   int64_t ir_len;
   int levels; /* levels held by LB */
   int base;   /* bitmap level of query level 0 */
+  uint32_t status; /* ORC_STATUS_* bits raised by the records */
 } qctx;
 
 /* The reference indexes file[] without bounds checks; on well-formed JSON it
@@ -277,9 +284,144 @@ static int read_varint(const qctx *c, int64_t *pos) {
   return (int)(value | (byte << shift));
 }
 
+
+/* ---- Extensions of this build (the reference rejects these queries) ----
+ *
+ * Numeric filter [?(@ <op> <number>)]: the value at the current position,
+ * trimmed of ' ' like EXPRESSION_STRING_EQUALS trims it (query.cu:414-441),
+ * must be a JSON number (RFC 8259 grammar) and compare as <op> against the
+ * literal; otherwise the record is abandoned.  The comparison is exact
+ * decimal arithmetic on the digit strings (no floating point): a number is
+ * 0.d1d2d3... x 10^E with d1 != 0, or zero; exponents saturate at +-10^15. */
+typedef struct {
+  int neg, zero;
+  int64_t E;       /* decimal exponent of 0.d1d2... */
+  int64_t nd;      /* significant digits (from the first nonzero digit) */
+  int64_t first;   /* index of the first significant digit in int+frac digits */
+  int64_t int_len; /* digits before the point */
+  const uint8_t *ip, *fp; /* integer and fraction digits */
+} orc_num;
+
+#define ORC_EXP_LIMIT 1000000000000000LL
+
+static int is_digit(uint8_t c) { return c >= '0' && c <= '9'; }
+
+static uint8_t num_digit(const orc_num *x, int64_t k) { /* k-th of int+frac digits */
+  return k < x->int_len ? x->ip[k] : x->fp[k - x->int_len];
+}
+
+/* Parses p[0..len) as one JSON number; 0 if it is not one. */
+static int num_parse(const uint8_t *p, int64_t len, orc_num *o) {
+  int64_t i = 0;
+  o->neg = 0;
+  if (i < len && p[i] == '-') {
+    o->neg = 1;
+    ++i;
+  }
+  if (i >= len) return 0;
+  const int64_t int_start = i;
+  if (p[i] == '0') {
+    ++i;
+  } else if (p[i] >= '1' && p[i] <= '9') {
+    while (i < len && is_digit(p[i])) ++i;
+  } else {
+    return 0;
+  }
+  o->ip = p + int_start;
+  o->int_len = i - int_start;
+  int64_t frac_len = 0;
+  o->fp = p + i;
+  if (i < len && p[i] == '.') {
+    ++i;
+    o->fp = p + i;
+    while (i < len && is_digit(p[i])) ++i;
+    frac_len = (p + i) - o->fp;
+    if (frac_len == 0) return 0;
+  }
+  int64_t ex = 0;
+  if (i < len && (p[i] == 'e' || p[i] == 'E')) {
+    ++i;
+    int eneg = 0;
+    if (i < len && (p[i] == '+' || p[i] == '-')) {
+      eneg = p[i] == '-';
+      ++i;
+    }
+    const int64_t es = i;
+    while (i < len && is_digit(p[i])) {
+      if (ex < ORC_EXP_LIMIT) ex = ex * 10 + (p[i] - '0');
+      ++i;
+    }
+    if (i == es) return 0;
+    if (ex > ORC_EXP_LIMIT) ex = ORC_EXP_LIMIT;
+    if (eneg) ex = -ex;
+  }
+  if (i != len) return 0;
+  const int64_t total = o->int_len + frac_len;
+  int64_t z = 0;
+  while (z < total && num_digit(o, z) == '0') ++z;
+  o->zero = z == total;
+  o->first = z;
+  o->nd = total - z;
+  o->E = o->int_len - z + ex;
+  return 1;
+}
+
+/* -1, 0, 1 as a <, ==, > b. */
+static int num_cmp(const orc_num *a, const orc_num *b) {
+  const int sa = a->zero ? 0 : (a->neg ? -1 : 1);
+  const int sb = b->zero ? 0 : (b->neg ? -1 : 1);
+  if (sa != sb) return sa < sb ? -1 : 1;
+  if (sa == 0) return 0;
+  int mag = 0;
+  if (a->E != b->E) {
+    mag = a->E > b->E ? 1 : -1;
+  } else {
+    const int64_t n = a->nd > b->nd ? a->nd : b->nd;
+    for (int64_t k = 0; k < n && mag == 0; ++k) {
+      const uint8_t da = k < a->nd ? num_digit(a, a->first + k) : '0';
+      const uint8_t db = k < b->nd ? num_digit(b, b->first + k) : '0';
+      if (da != db) mag = da > db ? 1 : -1;
+    }
+  }
+  return sa > 0 ? mag : -mag;
+}
+
+/* Comparators of OP_NUMBER_COMPARE. */
+enum { CMP_EQ = 0, CMP_NE = 1, CMP_LT = 2, CMP_LE = 3, CMP_GT = 4, CMP_GE = 5 };
+
+static int cmp_holds(int op, int r) {
+  switch (op) {
+  case CMP_EQ: return r == 0;
+  case CMP_NE: return r != 0;
+  case CMP_LT: return r < 0;
+  case CMP_LE: return r <= 0;
+  case CMP_GT: return r > 0;
+  case CMP_GE: return r >= 0;
+  default: return 0;
+  }
+}
+
+static int level_bit(const qctx *c, int level, int64_t pos) {
+  const int l = level + c->base;
+  if (l < 0 || l >= c->levels || pos < 0 || pos / 64 >= c->W) return 0;
+  return (int)((c->LB[(uint64_t)c->W * (uint64_t)l + (uint64_t)(pos / 64)] >> (pos % 64)) & 1u);
+}
+
+/* Does the string before the ':' at `colon` equal the key (the test of
+ * MOVE_TO_KEY, query.cu:254-302)? */
+static int key_matches(const qctx *c, int64_t line_start, int64_t colon, int64_t key_pos,
+                       int key_len) {
+  const int64_t string_end = find_previous_bitmap_bit(c->S, c->W, line_start + 1, colon - 1);
+  const int64_t string_start = string_end - key_len;
+  if (string_start < line_start || at(c, string_start) != '"') return 0;
+  for (int i = 0; i < key_len; ++i)
+    if (ir_at(c, key_pos + i) != at(c, string_start + i + 1)) return 0;
+  return 1;
+}
+
 /* One record: query.cu:150-451.  out points at this record's 2*num_results
  * slots, already filled with -1. */
-static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
+static void query_record(qctx *c, int64_t line_start, int64_t line_end,
                          int num_results, int64_t *out) {
   if (line_start < 0 || line_start >= c->n || line_end < 0) return;
   if (line_end >= c->n) line_end = c->n - 1;
@@ -328,6 +470,8 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
       if (num_results_index < num_results) {
         out[num_results_index * 2] = line_index;
         out[num_results_index * 2 + 1] = end_str;
+      } else {
+        c->status |= ORC_STATUS_OVERFLOW; /* only extension queries get here */
       }
       ++num_results_index;
       break;
@@ -508,6 +652,75 @@ static void query_record(const qctx *c, int64_t line_start, int64_t line_end,
       }
       break;
 
+    case OP_NUMBER_COMPARE: { /* extension: numeric filter */
+      const int cmp = ir_at(c, query_pos++);
+      const int lit_len = read_varint(c, &query_pos);
+      const int64_t lit_pos = query_pos;
+      query_pos += lit_len;
+      if (lit_len < 0 || lit_pos + lit_len > c->ir_len || !LEVEL_OK(current_level)) return;
+      while (at(c, line_index) == ' ' && line_index < level_end[current_level]) ++line_index;
+      int64_t value_end = level_end[current_level] - 1;
+      while (line_index < value_end && at(c, value_end) == ' ') --value_end;
+      if (line_index < 0 || value_end >= c->n || value_end < line_index) return;
+      orc_num v, lit;
+      if (!num_parse(c->in + line_index, value_end - line_index + 1, &v)) return;
+      if (!num_parse(c->ir + lit_pos, lit_len, &lit)) return;
+      if (!cmp_holds(cmp, num_cmp(&v, &lit))) return;
+      break;
+    }
+
+    case OP_DESCEND_KEY: { /* extension: "..name" as the last step */
+      key_len = read_varint(c, &query_pos);
+      key_pos = query_pos;
+      query_pos += key_len;
+      if (key_len < 0 || !LEVEL_OK(current_level)) return;
+      const int64_t hi = level_end[current_level];
+      /* every member named key inside the current value, at any level the
+       * index holds, in document order (by the position of its ':') */
+      for (int64_t p = line_index; p < hi; ++p) {
+        if (at(c, p) != ':') continue;
+        int lv = -1;
+        for (int l = current_level; l + c->base < c->levels; ++l) {
+          if (level_bit(c, l, p)) {
+            lv = l;
+            break;
+          }
+        }
+        if (lv < 0 || !key_matches(c, line_start, p, key_pos, key_len)) continue;
+        const int64_t vend = find_next_structural_char(c, hi, p + 1, lv);
+        int64_t vs = p + 1;
+        while (at(c, vs) == ' ' && vs < vend) ++vs;
+        int64_t ve = vend;
+        while (ve > vs && at(c, ve - 1) == ' ') --ve;
+        if (num_results_index < num_results) {
+          out[num_results_index * 2] = vs;
+          out[num_results_index * 2 + 1] = ve;
+        } else {
+          c->status |= ORC_STATUS_OVERFLOW;
+        }
+        ++num_results_index;
+      }
+      break;
+    }
+
+    case OP_EXPECT_AT_MOST: { /* extension: "[*]" bounded to K elements */
+      const int limit = read_varint(c, &query_pos);
+      if (limit < 0 || !LEVEL_OK(current_level)) return;
+      if (limit == 0 || at(c, line_index) != '[') break;
+      /* K commas at this level before the closing bracket: K+1 elements */
+      int64_t p = line_index;
+      int commas = 0;
+      steps = 0;
+      while (commas < limit) {
+        if (++steps > max_steps) break;
+        p = find_next_structural_char(c, level_end[current_level], p + 1, current_level);
+        if (at(c, p) != ',') break;
+        ++commas;
+      }
+      if (limit > 0 && commas >= limit) c->status |= ORC_STATUS_OVERFLOW;
+      break;
+    }
+
     default: /* the reference asserts; release builds fall through */
       break;
     }
@@ -520,7 +733,15 @@ int orc_query(const uint8_t *in, uint64_t n, const int64_t *NL,
               uint64_t num_lines, const uint64_t *S, const uint64_t *LB,
               uint64_t W, int num_levels, int base_level, const uint8_t *ir,
               uint64_t ir_len, int num_results, int64_t *out) {
-  qctx c = {in, (int64_t)n, S, LB, (int64_t)W, ir, (int64_t)ir_len, num_levels, base_level};
+  return orc_query_status(in, n, NL, num_lines, S, LB, W, num_levels, base_level, ir, ir_len,
+                          num_results, out, NULL);
+}
+
+int orc_query_status(const uint8_t *in, uint64_t n, const int64_t *NL,
+                     uint64_t num_lines, const uint64_t *S, const uint64_t *LB,
+                     uint64_t W, int num_levels, int base_level, const uint8_t *ir,
+                     uint64_t ir_len, int num_results, int64_t *out, uint32_t *status) {
+  qctx c = {in, (int64_t)n, S, LB, (int64_t)W, ir, (int64_t)ir_len, num_levels, base_level, 0u};
   for (uint64_t r = 0; r < num_lines; ++r) {
     int64_t *o = out + r * (uint64_t)num_results * 2u;
     for (int i = 0; i < 2 * num_results; ++i) o[i] = -1;
@@ -529,5 +750,6 @@ int orc_query(const uint8_t *in, uint64_t n, const int64_t *NL,
     const int64_t line_end = (r + 1 < num_lines) ? NL[r + 1] : (int64_t)n - 1;
     query_record(&c, line_start, line_end, num_results, o);
   }
+  if (status != NULL) *status = c.status;
   return 0;
 }

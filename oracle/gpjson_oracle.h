@@ -62,6 +62,18 @@ int orc_query(const uint8_t *in, uint64_t n, const int64_t *NL,
               uint64_t W, int num_levels, int base_level, const uint8_t *ir,
               uint64_t ir_len, int num_results, int64_t *out);
 
+/* orc_query that also returns status bits: ORC_STATUS_OVERFLOW when a record
+ * had more results than num_results (only the extension opcodes can: a
+ * recursive descent with more matches, or a "[*]" array longer than its
+ * limit).  Extensions of this build, rejected by the reference's compiler:
+ * 0x0A NUMBER_COMPARE (numeric filter), 0x0B DESCEND_KEY ("..name" as the
+ * last step), 0x0C EXPECT_AT_MOST ("[*]" element-count check). */
+#define ORC_STATUS_OVERFLOW 1u
+int orc_query_status(const uint8_t *in, uint64_t n, const int64_t *NL,
+                     uint64_t num_lines, const uint64_t *S, const uint64_t *LB,
+                     uint64_t W, int num_levels, int base_level, const uint8_t *ir,
+                     uint64_t ir_len, int num_results, int64_t *out, uint32_t *status);
+
 /* Reference-faithful serial escape state machine over one whole buffer with an
  * UNBOUNDED backslash-run carry (the test oracle is_escaped_quote rule of
  * tests/index/string_index_test.cpp:28-34).  Used only to show where the

@@ -8,6 +8,9 @@ compilation) and linked with the harness.  Nothing of the reference is copied
 into this repository.
 
     python oracle/ref/build_ref.py [reference_root]
+
+The reference checkout is the argument, else $GPJSON_REFERENCE_ROOT, else
+the read-only mount this recipe was written against.
 """
 from __future__ import annotations
 
@@ -23,8 +26,14 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
-def build(ref_root: str = "/root/reference", verbose: bool = False) -> Path | None:
-    ref = Path(ref_root)
+def reference_root() -> Path:
+    """Where the reference project's sources are read from (they are never
+    copied into this repository)."""
+    return Path(os.environ.get("GPJSON_REFERENCE_ROOT", "/root/reference"))
+
+
+def build(ref_root: str | None = None, verbose: bool = False) -> Path | None:
+    ref = Path(ref_root) if ref_root else reference_root()
     src = ref / "src" / "gpjson"
     if not src.is_dir():
         return None

@@ -2,7 +2,7 @@
 tests/golden/reference_kats.json.
 
 Run in a checkout where the reference project is available (its path is the
-first argument, default /root/reference).  Only the small literal fixtures and
+first argument, else $GPJSON_REFERENCE_ROOT, else /root/reference).  Only the small literal fixtures and
 expected values of the reference's unit tests are extracted:
 
   tests/index/newline_index_test.cpp        ComputesExpectedNewlineIndex
@@ -155,4 +155,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    import os
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else
+              os.environ.get("GPJSON_REFERENCE_ROOT", "/root/reference")))

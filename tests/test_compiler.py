@@ -12,7 +12,10 @@ import pytest
 KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
 OPS = {0: "END", 1: "STORE_RESULT", 2: "MOVE_UP", 3: "MOVE_DOWN", 4: "MOVE_TO_KEY",
        5: "MOVE_TO_INDEX", 6: "MOVE_TO_INDEX_REVERSE", 7: "MARK_POSITION",
-       8: "RESET_POSITION", 9: "EXPRESSION_STRING_EQUALS"}
+       8: "RESET_POSITION", 9: "EXPRESSION_STRING_EQUALS",
+       # extensions of this build (the reference rejects these queries)
+       10: "NUMBER_COMPARE", 11: "DESCEND_KEY", 12: "EXPECT_AT_MOST"}
+CMPS = {0: "==", 1: "!=", 2: "<", 3: "<=", 4: ">", 5: ">="}
 
 
 def decode(ir: bytes):
@@ -34,11 +37,14 @@ def decode(ir: bytes):
         op = OPS[ir[i]]
         i += 1
         ins = {"opcode": op}
-        if op in ("MOVE_TO_KEY", "EXPRESSION_STRING_EQUALS"):
+        if op == "NUMBER_COMPARE":
+            ins["cmp"] = CMPS[ir[i]]
+            i += 1
+        if op in ("MOVE_TO_KEY", "EXPRESSION_STRING_EQUALS", "NUMBER_COMPARE", "DESCEND_KEY"):
             n = varint()
             ins["string"] = ir[i:i + n].decode()
             i += n
-        elif op in ("MOVE_TO_INDEX", "MOVE_TO_INDEX_REVERSE"):
+        elif op in ("MOVE_TO_INDEX", "MOVE_TO_INDEX_REVERSE", "EXPECT_AT_MOST"):
             ins["integer"] = varint()
         out.append(ins)
         if op == "END":
@@ -123,9 +129,63 @@ def test_large_varint(gpj):
 
 
 def test_wildcard_extension_is_off_by_default(gpj):
-    with pytest.raises(gpj.UnsupportedQueryError):
+    with pytest.raises(gpj.UnsupportedQueryError, match="Unsupported wildcard expression"):
         gpj.compile("$.entities.hashtags[*].text")
     w = gpj.compile("$.entities.hashtags[*].text", wildcard_limit=8)
     r = gpj.compile("$.entities.hashtags[0:8].text")
-    assert (w.ir_bytes, w.max_depth, w.num_result_slots) == \
-        (r.ir_bytes, r.max_depth, r.num_result_slots)
+    # "[*]" = an element-count check, then exactly the IR of "[0:8]"
+    wi, ri = decode(w.ir_bytes), decode(r.ir_bytes)
+    assert wi[4] == {"opcode": "EXPECT_AT_MOST", "integer": 8}
+    assert wi[:4] + wi[5:] == ri
+    assert (w.max_depth, w.num_result_slots) == (r.max_depth, r.num_result_slots)
+
+
+def test_reference_syntax_never_uses_extension_opcodes(gpj):
+    for case in KATS["compiler"]["cases"]:
+        if "query" in case:
+            assert all(ins["opcode"] not in ("NUMBER_COMPARE", "DESCEND_KEY", "EXPECT_AT_MOST")
+                       for ins in decode(gpj.compile(case["query"]).ir_bytes))
+
+
+def test_recursive_descent_extension(gpj):
+    with pytest.raises(gpj.UnsupportedQueryError, match="Unsupported recursive descent at 2"):
+        gpj.compile("$..id")  # the reference's error without a slot limit
+    c = gpj.compile("$..id", wildcard_limit=5)
+    assert decode(c.ir_bytes) == [{"opcode": "DESCEND_KEY", "string": "id"}, {"opcode": "END"}]
+    assert (c.num_result_slots, c.max_depth) == (5, 15)
+    c = gpj.compile("$.user..id", wildcard_limit=3)
+    assert [i["opcode"] for i in decode(c.ir_bytes)] == \
+        ["MOVE_TO_KEY", "MOVE_DOWN", "DESCEND_KEY", "END"]
+    assert c.num_result_slots == 3
+    with pytest.raises(gpj.UnsupportedQueryError, match="after a recursive descent"):
+        gpj.compile("$..a.b", wildcard_limit=3)
+    with pytest.raises(gpj.MalformedQueryError, match="empty property"):
+        gpj.compile("$..", wildcard_limit=3)
+
+
+@pytest.mark.parametrize("text,cmp,lit", [("@ > 5", ">", "5"), ("@ >= -1.5e3", ">=", "-1.5e3"),
+                                          ("@ < 0.25", "<", "0.25"), ("@ <= 0", "<=", "0"),
+                                          ("@ != 12", "!=", "12"), ("@ == 7E+2", "==", "7E+2"),
+                                          ("@.b > 3", ">", "3")])
+def test_numeric_filter_extension(gpj, text, cmp, lit):
+    c = gpj.compile(f"$.a[?({text})]")
+    ins = decode(c.ir_bytes)
+    i = [k for k, x in enumerate(ins) if x["opcode"] == "NUMBER_COMPARE"][0]
+    assert ins[i] == {"opcode": "NUMBER_COMPARE", "cmp": cmp, "string": lit}
+    assert ins[i + 1] == {"opcode": "RESET_POSITION"}
+    assert ins[2] == {"opcode": "MARK_POSITION"}
+    assert c.num_result_slots == 1
+
+
+@pytest.mark.parametrize("query,err,msg", [
+    ('$.a[?(@ > "x")]', "UnsupportedQueryError", "comparison of a string"),
+    ("$.a[?(@ > 01)]", "MalformedQueryError", "Invalid number"),
+    ("$.a[?(@ > 1.)]", "MalformedQueryError", "Invalid number"),
+    ("$.a[?(@ > 1e)]", "MalformedQueryError", "Invalid number"),
+    ("$.a[?(@ > +1)]", "MalformedQueryError", "Invalid number"),
+    ("$.a[?(@ == x)]", "MalformedQueryError", "Invalid quoted string"),
+    ("$.a[?(@ ~ 1)]", "UnsupportedQueryError", "Unsupported character for expression"),
+])
+def test_filter_errors(gpj, query, err, msg):
+    with pytest.raises(getattr(gpj, err), match=msg):
+        gpj.compile(query)

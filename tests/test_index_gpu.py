@@ -168,3 +168,58 @@ def test_async_build_into_caller_buffers(cuda_ctx, gpj):
     np.testing.assert_array_equal(E.cpu().numpy().view(np.uint64), want.E)
     np.testing.assert_array_equal(Q.cpu().numpy().view(np.uint64), want.Q)
     np.testing.assert_array_equal(NL.cpu().numpy()[: want.num_lines], want.NL)
+
+
+def test_async_summary_is_four_words(cuda_ctx, gpj):
+    """gpj_index_build_async writes exactly d_summary[0..3] (lines, in-string,
+    depth, error bits): a guard word right after them stays untouched."""
+    import torch
+    from gpjson_b200 import datagen
+    guard = 0x5A5A5A5A5A5A5A5A
+    for data in (datagen.tweets(6, 100_000), np.zeros(0, np.uint8)):
+        n = data.size
+        t, ptr = to_device(data)
+        W = max(1, (n + 63) // 64)
+        S = torch.empty(W, dtype=torch.int64, device="cuda")
+        LB = torch.empty(W * 2, dtype=torch.int64, device="cuda")
+        NL = torch.empty(n // 16 + 16, dtype=torch.int64, device="cuda")
+        summ = torch.full((5,), guard, dtype=torch.int64, device="cuda")
+        ix = gpj.Index()
+        ix.d_string, ix.d_leveled = S.data_ptr(), LB.data_ptr()
+        ix.d_newline, ix.newline_capacity = NL.data_ptr(), NL.numel()
+        cuda_ctx.build_index_async(ptr, n, 2, ix, summ.data_ptr())
+        torch.cuda.synchronize()
+        s = summ.cpu().numpy()
+        want = oracle.OracleIndex(data, 2)
+        assert s[0] == want.num_lines and s[1] == 0 and s[2] == -1 and s[3] == 0
+        assert s[4] == guard
+
+
+def test_lookback_wait_runs_out_and_reports_timeout(cuda_ctx, gpj):
+    """A look-back whose predecessor never publishes (tile 0 left out of the
+    launch) gives up after a bounded number of polls: the kernel returns, the
+    error word carries the look-back bit, the host reports GPJ_ERR_TIMEOUT,
+    and the context keeps working for the next build."""
+    import torch
+    from gpjson_b200 import datagen
+    data = datagen.tweets(5, 8 * TILE)
+    n = data.size
+    t, ptr = to_device(data)
+    diag = gpj.GPJ_INDEX_DIAG_TILE0_UNPUBLISHED
+    with pytest.raises(gpj.DeviceTimeoutError, match="bounded wait"):
+        cuda_ctx.build_index(ptr, n, 2, diag)
+    W = (n + 63) // 64
+    S = torch.empty(W, dtype=torch.int64, device="cuda")
+    LB = torch.empty(W * 2, dtype=torch.int64, device="cuda")
+    NL = torch.empty(n // 16 + 16, dtype=torch.int64, device="cuda")
+    summ = torch.zeros(4, dtype=torch.int64, device="cuda")
+    ix = gpj.Index()
+    ix.d_string, ix.d_leveled = S.data_ptr(), LB.data_ptr()
+    ix.d_newline, ix.newline_capacity = NL.data_ptr(), NL.numel()
+    cuda_ctx.build_index_async(ptr, n, 2, ix, summ.data_ptr(), flags=diag)
+    torch.cuda.synchronize()
+    assert int(summ[3].item()) & 1  # look-back timeout bit
+    with pytest.raises(ValueError, match="two tiles"):
+        cuda_ctx.build_index(ptr, 1000, 2, diag)
+    # the same context, a normal build: bit-exact again
+    assert_same(gpu_index(cuda_ctx, gpj, data, 2), oracle.OracleIndex(data, 2))

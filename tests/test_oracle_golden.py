@@ -14,7 +14,19 @@ import oracle
 import ref_test_oracles as rto
 
 KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
-DATASETS = Path("/root/reference/dataset")
+
+
+def _reference_root() -> Path:
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_gpjb_build_ref", Path(__file__).resolve().parent.parent / "oracle" / "ref" / "build_ref.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.reference_root()
+
+
+# the reference's sample datasets, read in place where the reference is present
+DATASETS = _reference_root() / "dataset"
 
 
 def test_newline_kat():

@@ -44,6 +44,15 @@ def test_noalloc_matches_context_build(gpj, kind, size, offset):
     t, ptr = to_device(data, offset)
     stream = torch.cuda.current_stream().cuda_stream
 
+    # the warm-up a host that reserves all device memory makes before
+    # reserving: the first call looks up the scratch array's address (and
+    # CUDA's lazy loading places the module then)
+    warm = _buffers(0, levels, 1)
+    gpj.build_index_noalloc(ptr, 0, levels, _index(gpj, warm), warm["sum"].data_ptr(),
+                            stream=stream)
+    torch.cuda.synchronize()
+    assert warm["sum"].cpu().tolist() == [1, 0, -1, 0]
+
     ref = _buffers(n, levels, nl_cap)
     with gpj.Context(0) as ctx:
         ctx.build_index_async(ptr, n, levels, _index(gpj, ref), ref["sum"].data_ptr(),
