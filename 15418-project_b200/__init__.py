@@ -50,7 +50,7 @@ EXPORTED_SYMBOLS = (
     "gpj_compile", "gpj_index_build", "gpj_index_build_async", "gpj_index_build_noalloc",
     "gpj_index_free",
     "gpj_query_run", "gpj_query_run64", "gpj_query_run_opts", "gpj_query_host",
-    "gpj_query_status",
+    "gpj_query_status", "gpj_copy_to_device",
     "gpj_results_compact",
     "gpj_batch_create", "gpj_batch_run", "gpj_batch_run_stages", "gpj_batch_run_per_file",
     "gpj_batch_run_host",
@@ -236,6 +236,7 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_query_run_opts.argtypes = [vp, P(Index), vp, u64, u32, P(QueryOpts), vp, vp]
     lib.gpj_query_host.argtypes = [vp, vp, u64, i32, u32, vp, vp, vp, vp, vp, vp, P(u64), vp]
     lib.gpj_query_status.argtypes = [vp, P(u32), vp]
+    lib.gpj_copy_to_device.argtypes = [vp, vp, vp, u64, vp]
     lib.gpj_results_compact.argtypes = [vp, vp, u64, u32, vp, u64, C.c_int64, vp, u64, vp, u64,
                                         vp, vp]
     lib.gpj_batch_create.argtypes = [vp, vp, u64, P(BatchFile), u32, P(BatchQuery), u32, u32,
@@ -370,6 +371,13 @@ class Context:
         _check(self._lib.gpj_query_run_opts(self._h, C.byref(index), ir, len(compiled.ir_bytes),
                                             compiled.num_result_slots, C.byref(opts),
                                             C.c_void_p(d_out), C.c_void_p(stream)))
+
+    def copy_to_device(self, d_dst: int, h_src: int, size_bytes: int, stream: int = 0) -> None:
+        """gpj_copy_to_device: host -> device; pageable sources are staged
+        through the context's pinned ring (returns once the source may be
+        reused; the copy completes in stream order)."""
+        _check(self._lib.gpj_copy_to_device(self._h, C.c_void_p(d_dst), C.c_void_p(h_src),
+                                            size_bytes, C.c_void_p(stream)))
 
     def query_status(self, stream: int = 0) -> int:
         """gpj_query_status: status bits of this context's queries since the

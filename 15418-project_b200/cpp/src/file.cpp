@@ -2,6 +2,8 @@
 // src/gpjson/file/file_reader.cpp:18-77 and file.cpp:30-36).
 #include "gpjson/error/error.hpp"
 #include "gpjson/file/file_reader.hpp"
+#include "gpjson_b200.h"
+#include "internal.hpp"
 
 #include <fcntl.h>
 #include <sys/mman.h>
@@ -22,7 +24,12 @@ FilePartition::FilePartition(size_t partition_id, size_t start, size_t end, cons
 void FilePartition::load_to_device() {
   if (device_loaded()) return;
   device_data_ = cuda::DeviceArray(size_bytes());
-  device_data_.copy_from_host(host_data_, size_bytes());
+  // mmap'd and other pageable bytes go through the engine context's pinned
+  // staging ring (gpj_copy_to_device), not a synchronous pageable cudaMemcpy
+  error::throw_for_status(gpj_copy_to_device(detail::engine_context(), device_data_.data(),
+                                             host_data_, size_bytes(), nullptr),
+                          "load_to_device");
+  cuda::synchronize_and_check();
 }
 
 std::ostream &operator<<(std::ostream &os, FileReaderType type) {

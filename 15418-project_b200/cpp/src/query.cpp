@@ -126,7 +126,6 @@ BatchQueryResult QueryExecutor::execute_batch(const BatchCompiledQuery &queries,
   ix.num_words = (ix.size_bytes + 63) / 64;
   ix.num_levels = built.get_leveled_bitmap_index().num_levels();
 
-  const char *host = static_cast<const char *>(partition.host_bytes());
   const size_t base = partition.global_start_offset();
   for (size_t q = 0; q < queries.size(); ++q) {
     const auto total_t = prof.begin_nestedf("query %zu total", q);
@@ -149,27 +148,51 @@ BatchQueryResult QueryExecutor::execute_batch(const BatchCompiledQuery &queries,
         "query");
     cuda::synchronize_and_check();
     prof.end(kt);
-    std::vector<int32_t> host_res(count, -1);
+    // Compaction on the device (gpj_results_compact): only the matches and
+    // their bytes cross PCIe, not the int32[lines][slots][2] array.  A first
+    // pass counts them, the second writes them into exact buffers.
     auto ct = prof.begin("copy_result_to_host");
-    dev.copy_to_host(host_res.data(), count * sizeof(int32_t));
+    cuda::DeviceArray counts(3 * sizeof(uint64_t));
+    uint64_t cnt[3] = {0, 0, 0};
+    error::throw_for_status(
+        gpj_results_compact(ctx, dev.as<int32_t>(), uint64_t(num_lines), uint32_t(slots),
+                            ix.d_input, ix.size_bytes, int64_t(base), nullptr, 0, nullptr, 0,
+                            counts.as<uint64_t>(), nullptr),
+        "compact");
+    counts.copy_to_host(cnt, sizeof(cnt));
+    if (cnt[2] != 0) throw exec_error("Query kernel produced an invalid result range");
+    std::vector<gpj_match> matches(static_cast<size_t>(cnt[0]));
+    std::vector<char> arena(static_cast<size_t>(cnt[1]));
+    if (cnt[0] > 0) {
+      cuda::DeviceArray d_matches(static_cast<size_t>(cnt[0]) * sizeof(gpj_match));
+      cuda::DeviceArray d_arena(std::max<size_t>(1, static_cast<size_t>(cnt[1])));
+      error::throw_for_status(
+          gpj_results_compact(ctx, dev.as<int32_t>(), uint64_t(num_lines), uint32_t(slots),
+                              ix.d_input, ix.size_bytes, int64_t(base),
+                              d_matches.as<gpj_match>(), cnt[0], d_arena.as<uint8_t>(), cnt[1],
+                              counts.as<uint64_t>(), nullptr),
+          "compact");
+      d_matches.copy_to_host(matches.data(), matches.size() * sizeof(gpj_match));
+      if (!arena.empty()) d_arena.copy_to_host(arena.data(), arena.size());
+    }
     prof.end(ct);
     auto at = prof.begin("append_query_line_results");
+    // every line keeps one offset per slot, empty where nothing matched
+    // (query_executor_host.cu:80-119)
+    size_t m = 0;
     for (int line = 0; line < num_lines; ++line) {
       LineQueryResult lr;
-      for (size_t s = 0; s < slots; ++s) {
-        const int32_t a = host_res[size_t(line) * slots * 2 + s * 2];
-        const int32_t b = host_res[size_t(line) * slots * 2 + s * 2 + 1];
-        if (a < 0 || b < 0) {
+      for (size_t slot = 0; slot < slots; ++slot) {
+        if (m < matches.size() && matches[m].line == uint64_t(line) && matches[m].slot == slot) {
+          const gpj_match &g = matches[m++];
+          QueryOffset o;
+          o.start = size_t(g.start);
+          o.end = size_t(g.end);
+          o.json_text = std::string(arena.data() + g.text_offset, g.length);
+          lr.add_offset(std::move(o));
+        } else {
           lr.add_offset(QueryOffset{});
-          continue;
         }
-        if (a > b || size_t(b) > partition.size_bytes())
-          throw exec_error("Query kernel produced an invalid result range");
-        QueryOffset o;
-        o.start = base + size_t(a);
-        o.end = base + size_t(b);
-        o.json_text = std::string(host + a, size_t(b - a));
-        lr.add_offset(std::move(o));
       }
       result.add_line_result(q, std::move(lr));
     }

@@ -9,9 +9,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 
 struct gpj_ctx {
   int device = 0;
@@ -33,6 +35,11 @@ struct gpj_ctx {
   cudaEvent_t piece_ready = nullptr;
   // status bits the context's query launches raise (GPJ_QUERY_OVERFLOW)
   unsigned int *d_status = nullptr;
+  // pinned staging ring for pageable or mmap'd host inputs (created on first
+  // use): a slot is refilled once the copy that last read it has finished
+  void *stage = nullptr;
+  cudaEvent_t stage_done[3] = {nullptr, nullptr, nullptr};
+  int stage_next = 0;
 };
 
 namespace {
@@ -142,6 +149,75 @@ int enqueue_index(gpj_ctx *ctx, const uint8_t *in, uint64_t n, int levels,
   return GPJ_OK;
 }
 
+// ---- Host -> device copies -------------------------------------------------
+//
+// A pinned (page-locked or registered) source is copied by the DMA engines
+// directly.  A pageable or mmap'd source would make every cudaMemcpyAsync
+// synchronous and staged through the driver's small bounce buffer; instead it
+// goes through a ring of pinned chunks: host threads copy chunk k+1 into the
+// ring while chunk k crosses PCIe, one cudaMemcpyAsync per chunk.
+constexpr uint64_t kStageChunk = 32ull << 20;
+constexpr int kStageSlots = 3;
+constexpr int kStageThreads = 4;
+
+bool host_is_pinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy split over a few host threads (one thread copies ~10 GB/s, PCIe
+// Gen5 takes ~55)
+void parallel_memcpy(uint8_t *dst, const uint8_t *src, uint64_t n) {
+  if (n < (4ull << 20)) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  const uint64_t part = ((n + kStageThreads - 1) / kStageThreads + 4095u) & ~uint64_t(4095);
+  std::thread workers[kStageThreads - 1];
+  for (int t = 1; t < kStageThreads; ++t) {
+    const uint64_t off = uint64_t(t) * part;
+    if (off < n)
+      workers[t - 1] = std::thread(
+          [=] { std::memcpy(dst + off, src + off, std::min<uint64_t>(part, n - off)); });
+  }
+  std::memcpy(dst, src, std::min<uint64_t>(part, n));
+  for (auto &w : workers)
+    if (w.joinable()) w.join();
+}
+
+// Enqueues the copy of [h, h + n) to d on `stream`.  Pageable sources are
+// staged; when this returns, the source may be reused.
+int stage_copy(gpj_ctx *ctx, uint8_t *d, const uint8_t *h, uint64_t n, cudaStream_t stream,
+               bool pinned) {
+  if (n == 0) return GPJ_OK;
+  if (pinned) {
+    GPJ_CUDA(cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, stream), "copy input");
+    return GPJ_OK;
+  }
+  if (ctx->stage == nullptr) {
+    GPJ_CUDA(cudaMallocHost(&ctx->stage, kStageChunk * kStageSlots), "cudaMallocHost");
+    for (auto &e : ctx->stage_done)
+      GPJ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  auto *ring = static_cast<uint8_t *>(ctx->stage);
+  for (uint64_t off = 0; off < n; off += kStageChunk) {
+    const uint64_t len = std::min(kStageChunk, n - off);
+    const int slot = ctx->stage_next;
+    ctx->stage_next = (slot + 1) % kStageSlots;
+    GPJ_CUDA(cudaEventSynchronize(ctx->stage_done[slot]), "cudaEventSynchronize");
+    uint8_t *chunk = ring + uint64_t(slot) * kStageChunk;
+    parallel_memcpy(chunk, h + off, len);
+    GPJ_CUDA(cudaMemcpyAsync(d + off, chunk, len, cudaMemcpyHostToDevice, stream),
+             "copy staged input");
+    GPJ_CUDA(cudaEventRecord(ctx->stage_done[slot], stream), "cudaEventRecord");
+  }
+  return GPJ_OK;
+}
+
 // Pieces of a host input: copied in this many tiles at a time on the copy
 // stream, each piece indexed as soon as it has arrived, so the index of one
 // piece overlaps the copy of the next.
@@ -155,9 +231,10 @@ constexpr uint32_t kIngestPieceTiles = 1024;  // 32 MiB
 int enqueue_index_from_host(gpj_ctx *ctx, const uint8_t *h_in, uint8_t *d_in, uint64_t n,
                             int levels, const gpj_index &out, cudaStream_t stream) {
   const uint64_t piece = uint64_t(kIngestPieceTiles) * gpjb::kTileBytes;
+  const bool pinned = n > 0 && host_is_pinned(h_in);
   if (n <= piece) {
-    if (n > 0)
-      GPJ_CUDA(cudaMemcpyAsync(d_in, h_in, n, cudaMemcpyHostToDevice, stream), "copy input");
+    const int rc = stage_copy(ctx, d_in, h_in, n, stream, pinned);
+    if (rc != GPJ_OK) return rc;
     return enqueue_index(ctx, d_in, n, levels, 0u, out, stream);
   }
   if (ctx->copy_stream == nullptr)
@@ -190,9 +267,8 @@ int enqueue_index_from_host(gpj_ctx *ctx, const uint8_t *h_in, uint8_t *d_in, ui
     const uint32_t t1 = t0 + kIngestPieceTiles < L.num_tiles ? t0 + kIngestPieceTiles : L.num_tiles;
     const uint64_t b0 = uint64_t(t0) * gpjb::kTileBytes;
     const uint64_t b1 = uint64_t(t1) * gpjb::kTileBytes < n ? uint64_t(t1) * gpjb::kTileBytes : n;
-    GPJ_CUDA(cudaMemcpyAsync(d_in + b0, h_in + b0, b1 - b0, cudaMemcpyHostToDevice,
-                             ctx->copy_stream),
-             "copy input piece");
+    const int rc = stage_copy(ctx, d_in + b0, h_in + b0, b1 - b0, ctx->copy_stream, pinned);
+    if (rc != GPJ_OK) return rc;
     GPJ_CUDA(cudaEventRecord(ctx->piece_ready, ctx->copy_stream), "cudaEventRecord");
     GPJ_CUDA(cudaStreamWaitEvent(stream, ctx->piece_ready, 0), "cudaStreamWaitEvent");
     GPJ_CUDA(gpjb::index_clear_counter(L, stream), "cudaMemsetAsync");
@@ -361,6 +437,17 @@ int gpj_ctx_create(int device, gpj_ctx **out) {
   return GPJ_OK;
 }
 
+int gpj_copy_to_device(gpj_ctx *ctx, void *d_dst, const void *h_src, uint64_t size_bytes,
+                       void *stream_) {
+  int rc = bind_device(ctx);
+  if (rc != GPJ_OK) return rc;
+  if (size_bytes > 0 && (d_dst == nullptr || h_src == nullptr))
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "null buffer with nonzero size");
+  if (size_bytes == 0) return GPJ_OK;
+  return stage_copy(ctx, static_cast<uint8_t *>(d_dst), static_cast<const uint8_t *>(h_src),
+                    size_bytes, static_cast<cudaStream_t>(stream_), host_is_pinned(h_src));
+}
+
 int gpj_query_status(gpj_ctx *ctx, uint32_t *flags, void *stream_) {
   if (flags == nullptr) return fail(GPJ_ERR_INVALID_ARGUMENT, "null flags");
   int rc = bind_device(ctx);
@@ -385,6 +472,9 @@ int gpj_ctx_destroy(gpj_ctx *ctx) {
   cudaFree(ctx->d_status);
   cudaFreeHost(ctx->pinned);
   if (ctx->piece_ready) cudaEventDestroy(ctx->piece_ready);
+  for (auto &e : ctx->stage_done)
+    if (e) cudaEventDestroy(e);
+  if (ctx->stage) cudaFreeHost(ctx->stage);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   delete ctx;
   return GPJ_OK;

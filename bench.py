@@ -596,22 +596,34 @@ def reference_gpu(data, queries, records, levels, ours_index_ms, ours_query_ms):
     compiled from its own sources into oracle/_ref) timed on the same GPU and
     input with CUDA events.  Array-record workloads: the reference indexes the
     array file and runs the queries on its NDJSON normalisation (it has no
-    "$[*]").  Not a bench value of this engine: a comparison column."""
+    "$[*]").  Every input and query is first checked on the CPU against the
+    reference's device-assert conditions (tests/ref_guard.py); an input that
+    would trip one is not run.  Not a bench value of this engine: a
+    comparison column."""
+    import re
     import tempfile
+
+    import ref_guard
     if not REF_DUMP.exists():
         return {"unavailable": "oracle/_ref/ref_dump not built"}
+    pkg = entry.package()
     out = {"source": "reference library built from its own sources (oracle/ref/build_ref.py)",
            "ours_index_ms": round(ours_index_ms, 4), "ours_query_ms": round(ours_query_ms, 4)}
     with tempfile.TemporaryDirectory() as d:
         raw = Path(d) / "input.json"
         np.asarray(data).tofile(raw)
-        qfile, qtext = raw, list(queries)
+        qfile, qtext, qdata = raw, list(queries), np.asarray(data)
         if records == "array":
             b = bytes(np.asarray(data))
             elems = [ln.rstrip(b",") for ln in b.split(b"\n") if ln not in (b"[", b"]", b"")]
             qfile = Path(d) / "records.ndjson"
-            qfile.write_bytes(b"\n".join(elems) + b"\n")
+            qdata = np.frombuffer(b"\n".join(elems) + b"\n", np.uint8)
+            qfile.write_bytes(qdata.tobytes())
             qtext = ["$" + q[4:] if q.startswith("$[*]") else q for q in queries]
+        comp = [pkg.compile(q) for q in qtext]
+        bad = ref_guard.problems(data, [], levels) + ref_guard.problems(qdata, comp, levels)
+        if bad:
+            return {"unavailable": "input would trip a reference device assert: " + bad[0]}
         for name, builder in (("SHAREMEM", 3), ("COMBINED", 1)):
             env = dict(os.environ, REF_TIME_REPS="5")
             r = subprocess.run([str(REF_DUMP), str(raw), str(builder), str(levels),
@@ -620,7 +632,6 @@ def reference_gpu(data, queries, records, levels, ours_index_ms, ours_query_ms):
             q = subprocess.run([str(REF_DUMP), str(qfile), str(builder), str(levels),
                                 str(Path(d) / (name + "_q"))] + qtext,
                                capture_output=True, text=True, env=env, timeout=900)
-            import re
             mi = re.search(r"ms_index ([0-9.]+) ms_query ([0-9.]+)", r.stdout)
             mq = re.search(r"ms_index ([0-9.]+) ms_query ([0-9.]+)", q.stdout)
             if r.returncode != 0 or q.returncode != 0 or mi is None or mq is None:
@@ -628,7 +639,50 @@ def reference_gpu(data, queries, records, levels, ours_index_ms, ours_query_ms):
                 continue
             ms_i, ms_q = float(mi.group(1)), float(mq.group(2))
             out[name] = {"index_ms": round(ms_i, 3), "query_ms": round(ms_q, 3),
-                         "index_speedup_ours": round(ms_i / ours_index_ms, 2)}
+                         "index_speedup_ours": round(ms_i / ours_index_ms, 2),
+                         "query_speedup_ours": round(ms_q / ours_query_ms, 2)}
+    return out
+
+
+def reference_gpu_column(pkg, local):
+    """The reference-GPU column of the default line: the reference's SHAREMEM
+    and COMBINED builders and its query executor against this engine on the
+    same B200, on the c0 (64 MiB NDJSON, $.user.lang) and c1 (1 GiB array,
+    $[*].categoryPath[1:3].id) inputs -- single inputs the reference's
+    launch configuration handles (the c3 table has no reference counterpart:
+    one Engine::query per file would take minutes)."""
+    import torch
+    out = {}
+    for name in ("c0", "c1"):
+        data, queries, records, _ = workload(name, pkg)
+        comp = compile_all(pkg, queries)
+        levels = max(c.max_depth + base for c, base in comp)
+        dev = torch.device("cuda", local)
+        ctx = pkg.Context(local)
+        d_in = torch.from_numpy(data).to(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        t_i = t_q = 0.0
+        reps = 5
+        for k in range(reps + 2):
+            ev[0].record()
+            ix = ctx.build_index(d_in.data_ptr(), data.size, levels)
+            ev[1].record()
+            for c, base in comp:
+                o = torch.empty(ix.num_lines * c.num_result_slots * 2, dtype=torch.int32,
+                                device=dev)
+                ctx.query(ix, c, o.data_ptr(), base_level=base)
+            ev[2].record()
+            torch.cuda.synchronize()
+            ctx.free_index(ix)
+            if k >= 2:
+                t_i += ev[0].elapsed_time(ev[1])
+                t_q += ev[1].elapsed_time(ev[2])
+        ctx.close()
+        del d_in
+        torch.cuda.empty_cache()
+        out[name] = reference_gpu(data, queries, records, levels, t_i / reps, t_q / reps)
+        out[name]["ours_timing"] = "index build (gpj_index_build: launch, summary read, " \
+                                   "allocation) and queries, CUDA events"
     return out
 
 
@@ -710,6 +764,7 @@ def run_batch(args, world, rank, local):
         e2e.append(e0.elapsed_time(e1))
     assert torch.equal(h_out[: int(v.result_ints)], want)
     e2e_ms = allreduce_max(float(np.mean(e2e)), world)
+    ingestion = ingestion_rates(pkg, buf, d_buf, h_in, local)
 
     gb = allreduce_sum(float(total), world) / 1e9  # every rank indexes its own files
     peak, peak_kind = measured_peak_hbm()
@@ -745,7 +800,10 @@ def run_batch(args, world, rank, local):
                      "algorithmic_bytes_per_launch": b_index, "ms_per_launch": round(ms_index, 4),
                      "chain_achieved": round(chain, 1), "chain_frac": round(chain / peak, 4)},
         "index_ms": round(ms_index, 4), "query_ms": round(ms_query, 4), "clocks": clk,
+        "ingestion": ingestion,
     }
+    if rank == 0 and not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu_column(pkg, local)
     if rank == 0 and not args.no_cpu_baseline:
         # the CPU baseline leg: the oracle over every timed file on every host
         # thread, timed, and its results compared with the batch's (the
@@ -758,6 +816,37 @@ def run_batch(args, world, rank, local):
             f"one file per task on {threads} threads, one pass ({dt:.2f} s)"}
     batch.close()
     return line
+
+
+def ingestion_rates(pkg, buf, d_buf, h_in, local, nbytes: int = 2 << 30, reps: int = 3):
+    """Host -> device GB/s of the first `nbytes` of the batch input: pageable
+    memory through gpj_copy_to_device's pinned staging ring, pageable memory
+    by a plain copy (what a synchronous pageable cudaMemcpy gets, as the
+    reference's FilePartition::load_to_device does), and pinned memory.
+    Wall clock around each call plus a device synchronisation."""
+    import torch
+    n = min(nbytes, buf.size)
+    src = buf[:n]
+    dst = d_buf[:n]
+    ctx = pkg.Context(local)
+    out = {"bytes": n}
+
+    def rate(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return round(n / min(ts) / 1e9, 2)
+
+    out["pageable_staged_gbs"] = rate(lambda: ctx.copy_to_device(dst.data_ptr(), src.ctypes.data, n))
+    out["pageable_plain_gbs"] = rate(lambda: dst.copy_(torch.from_numpy(src)))
+    out["pinned_gbs"] = rate(lambda: dst.copy_(h_in[:n], non_blocking=True))
+    ctx.close()
+    return out
 
 
 def oracle_files(files, queries, threads: int | None = None, limit_bytes: int | None = None):
@@ -925,6 +1014,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true",
                     help="c0-c2: also time the reference's own library on the same GPU")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="c3: skip the reference-GPU column (c0 and c1 inputs)")
     ap.add_argument("--size-mib", type=int, default=None,
                     help="profiling: run the workload's generator at this size")
     args = ap.parse_args()

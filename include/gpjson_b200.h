@@ -153,6 +153,19 @@ int gpj_index_build_noalloc(const uint8_t *d_input, uint64_t size_bytes,
                             int num_levels, uint32_t flags, gpj_index *index,
                             uint64_t *d_summary, void *stream);
 
+/* Copies size_bytes of host memory to device memory on `stream`.  A pinned
+ * (page-locked or registered) source is one cudaMemcpyAsync.  A pageable or
+ * mmap'd source goes through the context's ring of three 32 MiB pinned
+ * chunks: host threads copy chunk k+1 into the ring while chunk k crosses
+ * PCIe, one cudaMemcpyAsync per chunk; the call returns once every chunk is
+ * staged (the source may then be reused) and the device copy completes in
+ * `stream` order.  gpj_query_host stages its pageable inputs the same way,
+ * piece by piece, overlapped with the indexing of the pieces before.
+ * Replaces the synchronous pageable copy of FilePartition::load_to_device
+ * (src/gpjson/file/file.cpp:30-36, src/gpjson/cuda/cuda.cpp:79-87). */
+int gpj_copy_to_device(gpj_ctx *ctx, void *d_dst, const void *h_src, uint64_t size_bytes,
+                       void *stream);
+
 /* Releases what gpj_index_build allocated. */
 int gpj_index_free(gpj_ctx *ctx, gpj_index *index);
 

@@ -98,9 +98,11 @@ class OracleIndex:
         assert got == lines
         self.num_lines = lines
 
-    # status bits of the last query (ORC_STATUS_OVERFLOW: a record had more
-    # results than slots -- only the extension opcodes can)
+    # status bits of the last query: ORC_STATUS_OVERFLOW, a record had more
+    # results than slots (only the extension opcodes can); ORC_STATUS_REF_ASSERT,
+    # a device assert of the reference's query kernel would fire on this input
     STATUS_OVERFLOW = 1
+    STATUS_REF_ASSERT = 2
     last_status = 0
 
     def query(self, ir: bytes, num_results: int, base_level: int = 0) -> np.ndarray:

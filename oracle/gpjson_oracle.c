@@ -454,6 +454,13 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
 /* The reference has no guard for these; the compiler never emits IR that
  * reaches them.  Leaving the record keeps the restatement memory safe. */
 #define LEVEL_OK(l) ((l) >= 0 && (l) < ORC_MAX_LEVELS)
+/* Where the reference's kernel has a device assert, the oracle records in
+ * the status that the condition failed (ORC_STATUS_REF_ASSERT) and carries
+ * on: test harnesses check it before handing an input to the reference. */
+#define REF_ASSERT(cond)                                                     \
+  do {                                                                       \
+    if (!(cond)) c->status |= ORC_STATUS_REF_ASSERT;                         \
+  } while (0)
 
   for (;;) {
     const uint8_t op = ir_at(c, query_pos++);
@@ -467,6 +474,7 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
       while (at(c, line_index) == ' ' && line_index < level_end[current_level])
         ++line_index;
       while (end_str > line_index && at(c, end_str - 1) == ' ') --end_str;
+      REF_ASSERT(line_index <= end_str); /* query.cu:230 */
       if (num_results_index < num_results) {
         out[num_results_index * 2] = line_index;
         out[num_results_index * 2 + 1] = end_str;
@@ -506,6 +514,7 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
           ++line_index;
           line_index = find_next_structural_char(c, level_end[current_level],
                                                  line_index, current_level);
+          REF_ASSERT(at(c, line_index) == ':' || at(c, line_index) == '}'); /* query.cu:265 */
           if (at(c, line_index) == ':') {
             const int64_t string_end = find_previous_bitmap_bit(
                 c->S, c->W, line_start + 1, line_index - 1);
@@ -525,6 +534,8 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
               ++line_index;
               line_index = find_next_structural_char(
                   c, level_end[current_level], line_index, current_level);
+              /* query.cu:276, 290 */
+              REF_ASSERT(at(c, line_index) == ',' || at(c, line_index) == '}');
               if (at(c, line_index) == '}') return;
               continue; /* goto search_key */
             }
@@ -552,6 +563,8 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
               ++line_index;
               line_index = find_next_structural_char(
                   c, level_end[current_level], line_index, current_level);
+              /* query.cu:321 */
+              REF_ASSERT(at(c, line_index) == ',' || at(c, line_index) == ']');
               if (at(c, line_index) == ',') {
                 ++curr_index[current_level];
                 continue;
@@ -562,6 +575,8 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
               --line_index;
               line_index =
                   find_previous_structural_char(c, 0, line_index, current_level);
+              /* query.cu:334 */
+              REF_ASSERT(at(c, line_index) == ',' || at(c, line_index) == '[');
               --curr_index[current_level];
               continue;
             }
@@ -592,6 +607,8 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
               --line_index;
               line_index =
                   find_previous_structural_char(c, 0, line_index, current_level);
+              /* query.cu:370 */
+              REF_ASSERT(at(c, line_index) == ',' || at(c, line_index) == '[');
               if (at(c, line_index) == ',' ||
                   curr_index[current_level] + 1 == target_index) {
                 ++curr_index[current_level];
@@ -603,6 +620,8 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
               ++line_index;
               line_index = find_next_structural_char(
                   c, level_end[current_level], line_index, current_level);
+              /* query.cu:384 */
+              REF_ASSERT(at(c, line_index) == ',' || at(c, line_index) == ']');
               --curr_index[current_level];
               continue;
             }
@@ -644,6 +663,8 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
       {
         int64_t string_end = level_end[current_level] - 1;
         while (line_index < string_end && at(c, string_end) == ' ') --string_end;
+        /* query.cu:430: a string filter on a value that is not a string */
+        REF_ASSERT(at(c, line_index) == '"' && at(c, string_end) == '"');
         const int64_t string_length = string_end - line_index + 1;
         if (string_length != key_len) return;
         for (int i = 0; i < key_len; ++i) {

@@ -69,6 +69,10 @@ int orc_query(const uint8_t *in, uint64_t n, const int64_t *NL,
  * 0x0A NUMBER_COMPARE (numeric filter), 0x0B DESCEND_KEY ("..name" as the
  * last step), 0x0C EXPECT_AT_MOST ("[*]" element-count check). */
 #define ORC_STATUS_OVERFLOW 1u
+/* A device assert of the reference's query kernel would fire on this input
+ * (src/gpjson/query/kernels/orig/query.cu:230, 265, 276, 290, 321, 334, 370,
+ * 384, 430); results are unaffected. */
+#define ORC_STATUS_REF_ASSERT 2u
 int orc_query_status(const uint8_t *in, uint64_t n, const int64_t *NL,
                      uint64_t num_lines, const uint64_t *S, const uint64_t *LB,
                      uint64_t W, int num_levels, int base_level, const uint8_t *ir,

@@ -6,7 +6,10 @@
 //   ref_dump <input> <builder 0..3> <levels> <out_prefix> [query ...]
 //
 // writes <out_prefix>.S (string index words), .LB (leveled bitmap words),
-// .NL (newline index, num_lines entries) and, per query q, .R<q> (int64
+// .NL (newline index, num_lines entries), .E and .Q (escape and quote
+// bitmap words from the SHAREMEM escape_carry_index -> escape_index ->
+// quote_index kernels, which the builders keep internal) and, per query q,
+// .R<q> (int64
 // [lines][slots][2], partition-local [start, end), -1 where a slot matched
 // nothing), built with IndexBuilderType <builder> (0 UNCOMBINED, 1 COMBINED,
 // 2 FUSED, 3 SHAREMEM) and <levels> leveled-bitmap levels (at least the
@@ -20,6 +23,7 @@
 #include "gpjson/file/file.hpp"
 #include "gpjson/file/file_reader.hpp"
 #include "gpjson/index/index_builder.hpp"
+#include "gpjson/index/kernels/sharemem.cuh"
 #include "gpjson/profiler/profiler.hpp"
 #include "gpjson/query/query_compiler.hpp"
 #include "gpjson/query/query_executor.hpp"
@@ -33,6 +37,7 @@
 #include <fstream>
 #include <iostream>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -86,6 +91,38 @@ int main(int argc, char **argv) {
     index::BuiltIndices built = builder->build(part, levels, opts.index_builder_options, ctx);
     cudaDeviceSynchronize();
 
+    // escape and quote bitmaps: the first three kernels of the SHAREMEM
+    // string index (sharemem_index_builder.cu:360-380, 219-229), one thread
+    // per 64-byte word, block 512
+    {
+      const int block = 512, grid = int(words / 512 + 1);
+      const size_t threads = size_t(grid) * size_t(block);
+      char *carry = nullptr, *qcarry = nullptr;
+      long *E = nullptr, *Q = nullptr;
+      cudaMalloc(&carry, threads);
+      cudaMalloc(&qcarry, threads);
+      cudaMalloc(&E, threads * sizeof(long));
+      cudaMalloc(&Q, threads * sizeof(long));
+      cudaMemset(E, 0, threads * sizeof(long));
+      cudaMemset(Q, 0, threads * sizeof(long));
+      const char *file = static_cast<const char *>(part.device_bytes());
+      index::kernels::sharemem::escape_carry_index<<<grid, block>>>(file, n, carry);
+      index::kernels::sharemem::escape_index<<<grid, block>>>(file, n, carry, E);
+      index::kernels::sharemem::quote_index<<<grid, block>>>(file, n, E, Q, qcarry);
+      const cudaError_t e = cudaDeviceSynchronize();
+      if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+      std::vector<int64_t> hE(words), hQ(words);
+      if (words) {
+        cudaMemcpy(hE.data(), E, words * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(hQ.data(), Q, words * 8, cudaMemcpyDeviceToHost);
+      }
+      write_raw(prefix + ".E", hE);
+      write_raw(prefix + ".Q", hQ);
+      cudaFree(carry);
+      cudaFree(qcarry);
+      cudaFree(E);
+      cudaFree(Q);
+    }
     write_raw(prefix + ".S", device_words(built.get_string_index()));
     write_raw(prefix + ".LB", device_words(built.get_leveled_bitmap_index()));
     std::vector<int64_t> nl = device_words(built.get_newline_index());

@@ -71,7 +71,7 @@ def test_descend_matches_json_walk(gpj, tweets, name):
     c = gpj.compile(f"$..{name}", wildcard_limit=64)
     ix = oracle.OracleIndex(tweets, c.max_depth)
     got = _values(tweets, ix.query(c.ir_bytes, c.num_result_slots))
-    assert ix.last_status == 0
+    assert not ix.last_status & oracle.OracleIndex.STATUS_OVERFLOW
     want = []
     for rec in _records(tweets):
         out = []
@@ -100,7 +100,7 @@ def test_descend_overflow_sets_status(gpj, tweets):
     c = gpj.compile("$..id", wildcard_limit=1)
     ix = oracle.OracleIndex(tweets, c.max_depth)
     res = ix.query(c.ir_bytes, c.num_result_slots)
-    assert ix.last_status == oracle.OracleIndex.STATUS_OVERFLOW
+    assert ix.last_status & oracle.OracleIndex.STATUS_OVERFLOW
     # the first match per record is still the first one in document order
     assert (res[:, 0, 0] >= 0).sum() > 0
 

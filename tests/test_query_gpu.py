@@ -186,3 +186,39 @@ def test_array_element_records(cuda_ctx, gpj, query):
     want = oracle.OracleIndex(data, L).query(c.ir_bytes, c.num_result_slots, 1)
     np.testing.assert_array_equal(got, want)
     assert (got[1:-1, 0, 0] >= 0).mean() > 0.5  # most elements match slot 0
+
+
+def test_copy_to_device_pageable_and_pinned(cuda_ctx, gpj):
+    """gpj_copy_to_device: a pageable source (several 32 MiB staging chunks,
+    an unaligned start) and a pinned one arrive bit for bit."""
+    rng = np.random.default_rng(5)
+    src = rng.integers(0, 256, (100 << 20) + 4099, dtype=np.uint8)
+    view = src[3:]  # pageable, unaligned
+    dst = torch.zeros(view.size + 16, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    cuda_ctx.copy_to_device(dst.data_ptr() + 1, view.ctypes.data, view.size, stream)
+    torch.cuda.synchronize()
+    got = dst.cpu().numpy()
+    assert np.array_equal(got[1:1 + view.size], view) and got[0] == 0 and got[-1] == 0
+    pinned = torch.from_numpy(src[: 5 << 20].copy()).pin_memory()
+    dst2 = torch.zeros(pinned.numel(), dtype=torch.uint8, device="cuda")
+    cuda_ctx.copy_to_device(dst2.data_ptr(), pinned.data_ptr(), pinned.numel(), stream)
+    torch.cuda.synchronize()
+    assert torch.equal(dst2.cpu(), pinned)
+
+
+def test_query_host_pageable_pieces(cuda_ctx, gpj):
+    """A pageable host input of more than one piece goes through the pinned
+    staging ring piece by piece; results equal the oracle's."""
+    data = _pieces_input()  # a numpy array: pageable memory
+    comp = [gpj.compile(q) for q in ["$.user.lang", "$.a"]]
+    L = max(c.max_depth for c in comp)
+    lines = data.tobytes().count(b"\n") + 1
+    outs = [np.full(lines * c.num_result_slots * 2, -9, np.int32) for c in comp]
+    got_lines = cuda_ctx.query_host(data.ctypes.data, data.size, L, comp,
+                                    [o.ctypes.data for o in outs], [o.size for o in outs])
+    assert got_lines == lines
+    want = oracle.OracleIndex(data, L)
+    for c, o in zip(comp, outs):
+        np.testing.assert_array_equal(o.astype(np.int64).reshape(lines, -1, 2),
+                                      want.query(c.ir_bytes, c.num_result_slots))

@@ -4,13 +4,15 @@ The reference library is compiled from its own sources into oracle/_ref by
 oracle/ref/build_ref.py and driven by the harness oracle/ref/ref_dump.cpp;
 for each of its four index builders (UNCOMBINED, COMBINED, FUSED, SHAREMEM)
 the string mask, leveled bitmaps, newline index and query results must equal
-this engine's bit for bit.  Inputs are well-formed JSON only: the
-reference's query search loops have no bound on malformed input, and its
-kernels assert on a few inputs (an all-backslash 64-byte chunk in
-escape_index; a non-string value under a string filter; the reverse-index
-walk over an empty array), so backslash runs stay below 64 bytes and the
-queries use forward indexes and no filters.  Skipped where oracle/_ref was
-not built (no reference sources at build time)."""
+this engine's bit for bit, and the escape and quote bitmaps of its SHAREMEM
+kernels (escape_index, quote_index) must equal this engine's E and Q.
+Inputs range from the reference's own fixtures to 64 MiB of post records
+(the c0 workload).  Inputs are well-formed JSON only: the reference's query
+search loops have no bound on malformed input, and its kernels assert on a
+few inputs, so every input and query is first checked on the CPU against
+those assert conditions (tests/ref_guard.py) and never reaches the reference
+if one would fire.  Skipped where oracle/_ref was not built (no reference
+sources at build time)."""
 import json
 import subprocess
 from pathlib import Path
@@ -20,6 +22,7 @@ import pytest
 import torch
 
 import oracle
+import ref_guard
 from devmem import to_device, index_arrays
 
 pytestmark = pytest.mark.gpu
@@ -64,6 +67,8 @@ def _inputs():
         # (tests/benchmark/benchmark_large_output_test.cpp:31-66) -- for queries
         "products_array_1MiB": (products, []),
         "products_ndjson_1MiB": (_as_ndjson(products), LINE_QUERIES),
+        "tweets_64MiB_c0": (bytes(datagen.tweets(0, 64 << 20)),
+                            ["$.user.lang", "$.entities.hashtags[0:8].text", "$.place.country_code"]),
     }
 
 
@@ -92,6 +97,8 @@ def test_reference_outputs_equal_ours(cases, builder, gpj, cuda_ctx):
     for name, (path, data, queries) in inputs.items():
         comp = [gpj.compile(q) for q in queries]
         levels = max([4] + [c.max_depth for c in comp])
+        # nothing reaches the reference's device asserts
+        assert ref_guard.problems(data, comp, levels) == [], name
         prefix = d / f"{name}.b{builder}"
         r = subprocess.run([str(REF), str(path), str(builder), str(levels), str(prefix)] + queries,
                            capture_output=True, text=True, timeout=300)
@@ -99,10 +106,14 @@ def test_reference_outputs_equal_ours(cases, builder, gpj, cuda_ctx):
         ref_S, ref_LB, ref_NL = (_read(f"{prefix}.{k}") for k in ("S", "LB", "NL"))
         b = oracle.as_bytes(data)
         t, ptr = to_device(b)
-        ix = cuda_ctx.build_index(ptr, b.size, levels)
+        ix = cuda_ctx.build_index(ptr, b.size, levels, gpj.GPJ_INDEX_EMIT_ESCAPE_QUOTE)
         try:
             ours = index_arrays(ix)
             W = (b.size + 63) // 64
+            np.testing.assert_array_equal(ours["E"].view(np.int64), _read(f"{prefix}.E")[:W],
+                                          err_msg=f"{name} E")
+            np.testing.assert_array_equal(ours["Q"].view(np.int64), _read(f"{prefix}.Q")[:W],
+                                          err_msg=f"{name} Q")
             np.testing.assert_array_equal(ours["S"].view(np.int64), ref_S[:W], err_msg=f"{name} S")
             np.testing.assert_array_equal(ours["LB"].view(np.int64), ref_LB[:W * levels],
                                           err_msg=f"{name} LB")
