@@ -165,6 +165,7 @@ class BatchView(C.Structure):
 
 GPJ_SERVER_NO_CACHE = 1
 GPJ_SERVER_SLEEP_POLL = 2
+GPJ_SERVER_NO_GROUPS = 4
 SERVER_MAX_QUERIES = 8
 
 
@@ -194,7 +195,7 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "submitted", "completed", "failed", "cache_hits", "cache_misses", "evictions", "rebuilds",
         "bytes_indexed", "bytes_served", "resident_indexes", "resident_bytes", "arena_used",
-        "arena_peak", "arena_bytes", "in_flight", "pending")]
+        "arena_peak", "arena_bytes", "in_flight", "pending", "index_launches")]
 
 
 _lib = None

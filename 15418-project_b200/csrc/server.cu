@@ -9,6 +9,14 @@
 //
 //   builder:  H2D input -> index kernel -> D2H summary  [event]
 //             -> queries -> D2H results                 [event] -> done
+//
+// Builds are batched: the cache-miss requests admitted in one scheduler pass
+// are indexed together by ONE file-table launch of the indexer (the batch
+// path's multi-file mode, with every file addressed inside the device
+// arena), followed by the per-file finalize kernel and one D2H of the file
+// rows; each request's resident index keeps its own input, string-mask and
+// leveled-bitmap block, and its newline index is a slice of the pass's
+// shared newline block, freed when the last of its residents goes.
 //   hit:      queries -> D2H results                    [event] -> done
 //   waiter:   (another request is building the same key) waits for that
 //             build, then runs its queries like a hit
@@ -133,6 +141,21 @@ class OffsetArena {
 
 struct Request;
 
+// One grouped build: the newline index of all its files (packed: file f at
+// its finalize row's slot), and a metadata block (file table, look-back
+// scratch, file rows, totals) with its pinned host mirror, freed once every
+// member has read its row.
+struct Group {
+  uint64_t nl_off = 0, nl_bytes = 0, nl_cap = 0;
+  int64_t *NL = nullptr;
+  uint64_t meta_off = 0, meta_bytes = 0;
+  uint64_t host_off = 0, host_bytes = 0;
+  const uint64_t *h_rows = nullptr;  // 8 words per file, then the 4 totals
+  uint32_t files = 0;
+  int pending = 0;  // members that have not read their row yet
+  int refs = 0;     // pending members + residents whose newline index lives here
+};
+
 // An index in the device arena: the input copy, string mask and leveled
 // bitmaps in one block, the newline index in another (shrunk to its exact
 // size once the line count is known).
@@ -142,6 +165,7 @@ struct Resident {
   int levels = 0;
   uint64_t main_off = 0, main_bytes = 0;
   uint64_t nl_off = 0, nl_bytes = 0, nl_cap = 0;
+  Group *nl_group = nullptr;  // newline index inside a grouped build's block
   uint8_t *d_input = nullptr;
   uint64_t *S = nullptr;
   uint64_t *LB = nullptr;
@@ -155,7 +179,7 @@ struct Resident {
   std::vector<Request *> waiters;
 };
 
-enum class St { Pending, Indexing, WaitIndex, WaitMemory, Querying, Done };
+enum class St { Pending, WaitGroup, Indexing, WaitIndex, WaitMemory, Querying, Done };
 
 struct Request {
   uint64_t id = 0;
@@ -171,6 +195,9 @@ struct Request {
   Resident *res = nullptr;
   bool builder = false;
   bool rebuild_pending = false;  // waiting for memory to rebuild a truncated NL
+  bool rebuild_copy = false;     // that rebuild must copy the input first
+  Group *group = nullptr;        // the grouped build indexing this request
+  uint32_t group_file = 0;       // its file (row) in that build
   bool wait_host = false;        // waiting for pinned result memory
   uint64_t work_off = 0, work_bytes = 0, scratch_bytes = 0, result_cap_ints = 0;
   bool has_work = false;
@@ -192,6 +219,12 @@ struct gpj_server {
   gpj_server_config cfg{};
   bool cache_on = true;
   bool sleep_poll = false;
+  bool group_builds = true;
+  // TMA view of the whole device arena (rows of 128 bytes) for grouped builds
+  CUtensorMap arena_map{};
+  bool arena_tma = false;
+  std::vector<Request *> tick;  // cache misses admitted in this pass, not built yet
+  std::unordered_map<Group *, std::unique_ptr<Group>> groups;
 
   uint8_t *d_arena = nullptr;
   OffsetArena dev;  // scheduler thread only
@@ -230,6 +263,22 @@ struct gpj_server {
       r->in_lru = false;
     }
   }
+  void unref_group(Group *g) {
+    if (--g->refs > 0) return;
+    if (g->nl_bytes) dev.release(g->nl_off, g->nl_bytes);
+    if (g->meta_bytes) dev.release(g->meta_off, g->meta_bytes);
+    if (g->host_bytes) host_free(g->host_off, g->host_bytes);
+    groups.erase(g);
+  }
+  // A member has read its row: the metadata block is done with once all have.
+  void group_row_read(Group *g) {
+    if (--g->pending == 0) {
+      if (g->meta_bytes) dev.release(g->meta_off, g->meta_bytes);
+      if (g->host_bytes) host_free(g->host_off, g->host_bytes);
+      g->meta_bytes = g->host_bytes = 0;
+    }
+    unref_group(g);
+  }
   void free_resident(Resident *r) {
     unlink_lru(r);
     if (r->key != 0) {
@@ -239,6 +288,10 @@ struct gpj_server {
     if (r->main_bytes) dev.release(r->main_off, r->main_bytes);
     if (r->nl_bytes) dev.release(r->nl_off, r->nl_bytes);
     r->main_bytes = r->nl_bytes = 0;
+    if (r->nl_group != nullptr) {
+      unref_group(r->nl_group);
+      r->nl_group = nullptr;
+    }
     {
       std::lock_guard<std::mutex> lk(mu);
       if (r->key != 0 && r->ready) {
@@ -394,6 +447,10 @@ struct gpj_server {
       fail_build(r, cuda_status(e), std::string("index build: ") + cudaGetErrorString(e));
       return false;
     }
+    if (res->size > 0) {
+      std::lock_guard<std::mutex> lk(mu);
+      stats.index_launches++;
+    }
     r->state = St::Indexing;
     return true;
   }
@@ -494,6 +551,10 @@ struct gpj_server {
   // the queries of the builder and of every request waiting for it.
   void on_index_done(Request *r) {
     Resident *res = r->res;
+    if (r->group != nullptr) {
+      on_group_member_done(r);
+      return;
+    }
     const unsigned long long *p = slots[r->slot].pinned;
     const uint64_t lines = p[0];
     const uint32_t err = reinterpret_cast<const uint32_t *>(p)[9];
@@ -519,6 +580,51 @@ struct gpj_server {
       dev.shrink(res->nl_off, res->nl_bytes, lines * 8u);
       res->nl_bytes = block_size(lines * 8u);
     }
+    publish_index(r, lines);
+  }
+
+  // A member of a grouped build: its row of the finalize output gives its
+  // line count and newline slot; the totals give the launch's error bits and
+  // the newline slots the group needed.
+  void on_group_member_done(Request *r) {
+    Resident *res = r->res;
+    Group *g = r->group;
+    r->group = nullptr;
+    const uint64_t *row = g->h_rows + uint64_t(r->group_file) * 8u;
+    const uint64_t *tot = g->h_rows + uint64_t(g->files) * 8u;
+    const uint64_t lines = row[gpjb::kFiLines];
+    const uint64_t err = tot[gpjb::kTotError];
+    if (err != 0) {
+      group_row_read(g);
+      fail_build(r, GPJ_ERR_TIMEOUT,
+                 "grouped index build: a bounded wait gave up (error bits " + std::to_string(err) +
+                     ")");
+      return;
+    }
+    if (tot[gpjb::kTotNlSlots] > g->nl_cap) {
+      // the group's newline block was too small: this member's index is
+      // built again on its own with its exact line count
+      group_row_read(g);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        stats.rebuilds++;
+      }
+      res->nl_cap = lines;
+      r->rebuild_pending = true;
+      retry_rebuild(r);
+      return;
+    }
+    res->NL = g->NL + row[gpjb::kFiNlOff];
+    res->nl_group = g;
+    g->refs++;  // held by the resident until it is freed
+    group_row_read(g);
+    publish_index(r, lines);
+  }
+
+  // The index of a builder is complete: publish it and start the queries of
+  // the builder and of every request waiting for it.
+  void publish_index(Request *r, uint64_t lines) {
+    Resident *res = r->res;
     res->lines = lines;
     res->ready = true;
     if (res->key != 0) {
@@ -548,7 +654,9 @@ struct gpj_server {
     res->nl_bytes = block_size(res->nl_cap * 8u);
     res->NL = reinterpret_cast<int64_t *>(dptr(off));
     r->rebuild_pending = false;
-    enqueue_build(r, false);
+    const bool copy = r->rebuild_copy;
+    r->rebuild_copy = false;
+    enqueue_build(r, copy);
   }
 
   // 1: admitted (or finished with an error), 0: does not fit yet.
@@ -583,6 +691,9 @@ struct gpj_server {
     const uint64_t lines_guess = build ? nl_cap : (res->ready ? res->lines : res->nl_cap);
     const uint64_t ints = lines_guess * r->slots_total * 2u;
     const uint64_t work_bytes = block_size(scratch + ints * 4u);
+    // a build of this pass is grouped with the others: its newline index goes
+    // to the group's shared block, allocated when the pass ends
+    const bool grouped = build && group_builds;
     const uint64_t need = work_bytes + (build ? main_bytes + block_size(nl_cap * 8u) : 0u);
     if (need > dev.size()) {
       finish(r, GPJ_ERR_OOM,
@@ -602,12 +713,12 @@ struct gpj_server {
     uint64_t main_off = 0, nl_off = 0, work_off = 0, host_off = 0;
     bool ok_main = !build, ok_nl = !build, ok_work = false, ok_host = false;
     if (build) ok_main = dev_alloc(main_bytes, &main_off);
-    if (build && ok_main) ok_nl = dev_alloc(nl_cap * 8u, &nl_off);
+    if (build && ok_main) ok_nl = grouped || dev_alloc(nl_cap * 8u, &nl_off);
     if (ok_main && ok_nl) ok_work = dev_alloc(work_bytes, &work_off);
     if (ok_work) ok_host = host_alloc(ints * 4u, &host_off);
     if (!ok_host) {
       if (ok_work) dev_free(work_off, work_bytes);
-      if (build && ok_nl) dev_free(nl_off, nl_cap * 8u);
+      if (build && ok_nl && !grouped) dev_free(nl_off, nl_cap * 8u);
       if (build && ok_main) dev_free(main_off, main_bytes);
       if (!build) {
         res->refs--;
@@ -647,13 +758,13 @@ struct gpj_server {
       res->main_off = main_off;
       res->main_bytes = main_bytes;
       res->nl_off = nl_off;
-      res->nl_bytes = block_size(nl_cap * 8u);
+      res->nl_bytes = grouped ? 0u : block_size(nl_cap * 8u);
       res->nl_cap = nl_cap;
       res->W = W;
       res->d_input = dptr(main_off);
       res->S = reinterpret_cast<uint64_t *>(dptr(main_off + in_bytes));
       res->LB = reinterpret_cast<uint64_t *>(dptr(main_off + in_bytes + s_bytes));
-      res->NL = reinterpret_cast<int64_t *>(dptr(nl_off));
+      res->NL = grouped ? nullptr : reinterpret_cast<int64_t *>(dptr(nl_off));
       res->refs = 1;
       if (cacheable) cache[r->key] = res;
       r->res = res;
@@ -663,7 +774,12 @@ struct gpj_server {
         stats.cache_misses++;
         stats.bytes_indexed += n;
       }
-      enqueue_build(r, true);
+      if (grouped) {
+        r->state = St::WaitGroup;
+        tick.push_back(r);
+      } else {
+        enqueue_build(r, true);
+      }
     } else {
       r->res = res;
       r->resp.cache_hit = 1;
@@ -743,7 +859,146 @@ struct gpj_server {
       }
       any = true;
     }
+    flush_tick();
     return any;
+  }
+
+  // ---- grouped builds --------------------------------------------------------
+  // A build that leaves the group path: its own newline block, then the
+  // single-file launch (or a wait for memory, retried by advance()).
+  void build_alone(Request *r) {
+    Resident *res = r->res;
+    uint64_t off = 0;
+    if (!dev_alloc(res->nl_cap * 8u, &off)) {
+      r->rebuild_pending = true;
+      r->rebuild_copy = true;
+      r->state = St::WaitMemory;
+      return;
+    }
+    res->nl_off = off;
+    res->nl_bytes = block_size(res->nl_cap * 8u);
+    res->NL = reinterpret_cast<int64_t *>(dptr(off));
+    enqueue_build(r, true);
+  }
+
+  void flush_tick() {
+    if (tick.empty()) return;
+    std::vector<Request *> members;
+    members.swap(tick);
+    if (members.size() == 1 || !enqueue_group(members))
+      for (Request *r : members) build_alone(r);
+  }
+
+  // Indexes every member with one file-table launch on the first member's
+  // stream: H2D of the inputs and the file table, indexer, finalize, one D2H
+  // of the file rows and totals; every member's event is recorded after it.
+  // false: no memory for the group's blocks (nothing was enqueued).
+  bool enqueue_group(const std::vector<Request *> &members) {
+    const uint32_t G = uint32_t(members.size());
+    uint64_t tiles = 0, nl_cap = 0;
+    int levels = 0;
+    for (Request *r : members) {
+      tiles += gpjb::tiles_for(r->res->size, gpjb::kIndexThreads);
+      nl_cap += r->res->nl_cap;
+      levels = std::max(levels, r->res->levels);
+    }
+    const uint64_t files_bytes = align_up(uint64_t(G) * sizeof(gpjb::IndexFile));
+    const uint64_t scratch_bytes = align_up(tiles * 8u + 64u);
+    const uint64_t rows_bytes = uint64_t(G) * 64u + 32u;
+    const uint64_t meta_bytes = files_bytes + scratch_bytes + align_up(rows_bytes);
+    const uint64_t host_bytes = files_bytes + align_up(rows_bytes);
+    auto owned = std::make_unique<Group>();
+    Group *g = owned.get();
+    bool ok = dev_alloc(nl_cap * 8u, &g->nl_off);
+    if (ok) g->nl_bytes = block_size(nl_cap * 8u);
+    ok = ok && dev_alloc(meta_bytes, &g->meta_off);
+    if (ok) g->meta_bytes = block_size(meta_bytes);
+    ok = ok && host_alloc(host_bytes, &g->host_off);
+    if (ok) g->host_bytes = block_size(host_bytes);
+    if (!ok) {
+      if (g->nl_bytes) dev_free(g->nl_off, g->nl_bytes);
+      if (g->meta_bytes) dev_free(g->meta_off, g->meta_bytes);
+      return false;
+    }
+    g->nl_cap = nl_cap;
+    g->NL = reinterpret_cast<int64_t *>(dptr(g->nl_off));
+    g->files = G;
+    auto *h_files = reinterpret_cast<gpjb::IndexFile *>(
+        reinterpret_cast<uint8_t *>(h_arena) + g->host_off);
+    g->h_rows = reinterpret_cast<const uint64_t *>(
+        reinterpret_cast<uint8_t *>(h_arena) + g->host_off + files_bytes);
+    uint64_t first = 0;
+    for (uint32_t f = 0; f < G; ++f) {
+      const Resident *res = members[f]->res;
+      gpjb::IndexFile F;
+      F.in_off = res->main_off;
+      F.n = res->size;
+      F.s_off = uint64_t(reinterpret_cast<uint8_t *>(res->S) - d_arena) / 8u;
+      F.lb_off = uint64_t(reinterpret_cast<uint8_t *>(res->LB) - d_arena) / 8u;
+      F.first_tile = uint32_t(first);
+      F.levels = res->levels;
+      h_files[f] = F;
+      first += gpjb::tiles_for(res->size, gpjb::kIndexThreads);
+    }
+    auto *d_files = reinterpret_cast<gpjb::IndexFile *>(dptr(g->meta_off));
+    auto *d_rows = reinterpret_cast<uint64_t *>(dptr(g->meta_off + files_bytes + scratch_bytes));
+    gpjb::IndexLaunch L;
+    L.in = d_arena;
+    L.full_rows = dev.size() / 128u;
+    L.files = d_files;
+    L.num_files = G;
+    L.num_levels = levels;
+    L.S = reinterpret_cast<uint64_t *>(d_arena);
+    L.LB = reinterpret_cast<uint64_t *>(d_arena);
+    L.NL = g->NL;
+    L.nl_cap = nl_cap;
+    L.num_tiles = uint32_t(tiles);
+    gpjb::index_bind_scratch(L, dptr(g->meta_off + files_bytes));
+    Slot &s = slots[members[0]->slot];
+    cudaError_t e = cudaSuccess;
+    for (Request *r : members)
+      if (e == cudaSuccess && r->res->size > 0)
+        e = cudaMemcpyAsync(r->res->d_input, r->h_input, r->res->size, cudaMemcpyHostToDevice,
+                            s.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_files, h_files, uint64_t(G) * sizeof(gpjb::IndexFile),
+                          cudaMemcpyHostToDevice, s.stream);
+    if (e == cudaSuccess && tiles > 0)
+      e = gpjb::index_launch(L, arena_tma ? &arena_map : nullptr, arena_tma, s.stream);
+    if (e == cudaSuccess && tiles == 0)
+      e = gpjb::index_clear_scratch(L, s.stream);
+    if (e == cudaSuccess)
+      e = gpjb::index_finalize_files(L, nullptr, nullptr, d_rows, d_rows + uint64_t(G) * 8u,
+                                     s.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(const_cast<uint64_t *>(g->h_rows), d_rows, rows_bytes,
+                          cudaMemcpyDeviceToHost, s.stream);
+    for (Request *r : members) {
+      if (e == cudaSuccess) e = cudaEventRecord(slots[r->slot].event, s.stream);
+    }
+    groups.emplace(g, std::move(owned));
+    g->pending = int(G);
+    g->refs = int(G);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stats.index_launches++;
+    }
+    for (uint32_t f = 0; f < G; ++f) {
+      Request *r = members[f];
+      r->group = g;
+      r->group_file = f;
+      r->state = St::Indexing;
+    }
+    if (e != cudaSuccess) {
+      const std::string msg = std::string("grouped index build: ") + cudaGetErrorString(e);
+      const int code = cuda_status(e);
+      for (Request *r : members) {
+        r->group = nullptr;
+        group_row_read(g);
+        fail_build(r, code, msg);
+      }
+    }
+    return true;
   }
 
   void clear_idle() {
@@ -833,6 +1088,7 @@ int gpj_server_create(const gpj_server_config *config, gpj_server **out) {
   s->cfg = cfg;
   s->cache_on = (cfg.flags & GPJ_SERVER_NO_CACHE) == 0;
   s->sleep_poll = (cfg.flags & GPJ_SERVER_SLEEP_POLL) != 0;
+  s->group_builds = (cfg.flags & GPJ_SERVER_NO_GROUPS) == 0;
   std::string err;
   int code = GPJ_OK;
   cudaError_t e = cudaMalloc(&s->d_arena, cfg.hbm_budget_bytes);
@@ -885,6 +1141,9 @@ int gpj_server_create(const gpj_server_config *config, gpj_server **out) {
   }
   s->dev.reset(cfg.hbm_budget_bytes);
   s->host.reset(cfg.host_result_bytes);
+  // grouped builds read every file inside the arena through one TMA view
+  s->arena_tma = gpjb::index_make_tensor_map(&s->arena_map, s->d_arena, s->dev.size(),
+                                             gpjb::kIndexThreads);
   s->stats.arena_bytes = s->dev.size();
   s->thread = std::thread([s] { s->loop(); });
   cudaSetDevice(prev);

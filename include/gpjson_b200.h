@@ -367,7 +367,10 @@ int gpj_batch_destroy(gpj_batch *batch);
 /* ---- Serving: continuous batching with resident indexes ------------------
  *
  * A server owns one device arena (the HBM budget), one pinned host arena for
- * results, and num_slots CUDA streams.  A scheduler thread admits submitted
+ * results, and num_slots CUDA streams.  The cache misses admitted in one
+ * scheduler pass are indexed by ONE launch of the multi-file indexer over the
+ * arena (then each request's queries run on its own stream);
+ * GPJ_SERVER_NO_GROUPS builds each with its own launch instead.  A scheduler thread admits submitted
  * requests in arrival order whenever a slot is free and the request's device
  * footprint (input copy, bitmaps, newline index, scratch, results) fits the
  * arena, evicting idle resident indexes least-recently-used first.  Admitted
@@ -385,6 +388,7 @@ typedef struct gpj_server gpj_server;
 
 #define GPJ_SERVER_NO_CACHE 1u /* never keep indexes resident */
 #define GPJ_SERVER_SLEEP_POLL 2u /* scheduler sleeps between event polls */
+#define GPJ_SERVER_NO_GROUPS 4u  /* build each cache miss with its own launch */
 #define GPJ_SERVER_MAX_QUERIES 8
 
 typedef struct gpj_server_config {
@@ -441,6 +445,7 @@ typedef struct gpj_server_stats {
   uint64_t resident_indexes, resident_bytes;
   uint64_t arena_used, arena_peak, arena_bytes;
   uint64_t in_flight, pending;
+  uint64_t index_launches;     /* indexer launches (a grouped build is one) */
 } gpj_server_stats;
 
 int gpj_server_create(const gpj_server_config *config, gpj_server **out);

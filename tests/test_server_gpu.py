@@ -184,3 +184,41 @@ def test_oversized_request_fails_and_others_finish(gpj):
     assert ra.status == gpj.GPJ_ERR_OOM and "budget" in ra.message
     assert rb.status == 0
     np.testing.assert_array_equal(rb.results[0].astype(np.int64), _oracle(small, c, 0, 2))
+
+
+def test_grouped_builds_equal_single_builds(gpj):
+    """Cache misses admitted in one scheduler pass are indexed by one
+    multi-file launch over the arena: fewer index launches than builds, and
+    every result equals a server that builds each file alone (and the
+    oracle), including a group whose shared newline block is too small (a
+    file of very short lines) and empty files."""
+    _need_gpu()
+    compiled = _compiled(gpj)
+    files = _files()
+    files.append(("t", np.frombuffer(b'{"a":1}\n{}\n' * 20000, np.uint8).copy()))
+    reqs = _requests(files, compiled, 40, seed=11)
+
+    def run(flags):
+        with gpj.Server(num_slots=32, hbm_budget_bytes=512 << 20, flags=flags) as s:
+            got = _run(s, reqs, one_at_a_time=False)
+            return got, s.stats()
+
+    grouped, st_g = run(0)
+    alone, st_a = run(gpj.GPJ_SERVER_NO_GROUPS)
+    assert st_g["failed"] == 0 and st_a["failed"] == 0
+    assert st_g["index_launches"] < st_g["cache_misses"], st_g
+    assert st_a["index_launches"] >= st_a["cache_misses"] - 2, st_a  # empty files launch nothing
+    assert st_g["rebuilds"] >= 1
+    for i, (key, data, qs, names) in enumerate(reqs):
+        g, a = grouped[i], alone[i]
+        assert g.status == 0 and a.status == 0, (g.message, a.message)
+        assert g.num_lines == a.num_lines
+        for (c, base, lv), qg, qa in zip(qs, g.results, a.results):
+            np.testing.assert_array_equal(qg, qa, err_msg=f"request {i}")
+    for fi, (kind, data) in enumerate(files):
+        for i, (key, d, qs, names) in enumerate(reqs):
+            if key == fi + 1:
+                c, base, lv = qs[0]
+                np.testing.assert_array_equal(grouped[i].results[0].astype(np.int64),
+                                              _oracle(data, c, base, lv), err_msg=f"file {fi}")
+                break
