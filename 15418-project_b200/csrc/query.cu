@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(256)
     // batch files are below 2 GiB (int32 results): 32-bit positions
     const Rec<int32_t> c{q.in + F.in_off, int32_t(F.n), q.S + F.s_off, q.LB + F.lb_off,
                          int32_t((F.n + 63u) / 64u), s_ir + g.ir_off, g.ir_len, g.base_level,
-                         F.levels, q.status};
+                         F.levels, q.file_status ? q.file_status + lo : q.status};
     run_record<int32_t, int32_t, kExt>(c, L, int32_t(start), int32_t(end), g.num_results, o);
   }
 }

@@ -72,6 +72,7 @@ struct BatchQueryLaunch {
   const uint64_t *totals = nullptr;
   int32_t *out = nullptr;
   unsigned int *status = nullptr;  // kQueryStatusOverflow is OR-ed here (optional)
+  unsigned int *file_status = nullptr;  // or into one word per file (optional, first)
   int num_groups = 0;
   BatchQueryGroup groups[kMaxBatchGroups];
 };

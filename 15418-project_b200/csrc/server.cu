@@ -179,7 +179,18 @@ struct Resident {
   std::vector<Request *> waiters;
 };
 
-enum class St { Pending, WaitGroup, Indexing, WaitIndex, WaitMemory, Querying, Done };
+enum class St { Pending, WaitGroup, Indexing, WaitIndex, WaitMemory, QueryReady, Querying, Done };
+
+// One batched query launch: every query of every request whose index became
+// ready in the same scheduler pass runs in ONE launch of the multi-file query
+// kernel; each (request, query) pair is one "file" of its table.  Its device
+// metadata (file table, file rows, totals, one status word per pair) and the
+// pinned host mirror are freed when the last of its requests finishes.
+struct QBatch {
+  uint64_t meta_off = 0, meta_bytes = 0;
+  uint64_t host_off = 0, host_bytes = 0;
+  int refs = 0;
+};
 
 struct Request {
   uint64_t id = 0;
@@ -198,6 +209,8 @@ struct Request {
   bool rebuild_copy = false;     // that rebuild must copy the input first
   Group *group = nullptr;        // the grouped build indexing this request
   uint32_t group_file = 0;       // its file (row) in that build
+  QBatch *qbatch = nullptr;      // the batched query launch running its queries
+  uint32_t status_words = 0;     // its per-query status words in the slot's pinned words
   bool wait_host = false;        // waiting for pinned result memory
   uint64_t work_off = 0, work_bytes = 0, scratch_bytes = 0, result_cap_ints = 0;
   bool has_work = false;
@@ -225,6 +238,8 @@ struct gpj_server {
   bool arena_tma = false;
   std::vector<Request *> tick;  // cache misses admitted in this pass, not built yet
   std::unordered_map<Group *, std::unique_ptr<Group>> groups;
+  std::vector<Request *> qready;  // requests whose queries run in this pass's batch
+  std::unordered_map<QBatch *, std::unique_ptr<QBatch>> qbatches;
 
   uint8_t *d_arena = nullptr;
   OffsetArena dev;  // scheduler thread only
@@ -356,7 +371,21 @@ struct gpj_server {
       res->in_lru = true;
     }
   }
+  void unref_qbatch(QBatch *b) {
+    if (--b->refs > 0) return;
+    if (b->meta_bytes) dev_free(b->meta_off, b->meta_bytes);
+    if (b->host_bytes) host_free(b->host_off, b->host_bytes);
+    qbatches.erase(b);
+  }
   void finish(Request *r, int status, const std::string &msg) {
+    if (r->qbatch != nullptr) {
+      unref_qbatch(r->qbatch);
+      r->qbatch = nullptr;
+    }
+    {
+      auto it = std::find(qready.begin(), qready.end(), r);
+      if (it != qready.end()) qready.erase(it);
+    }
     release_work(r);
     if (status != GPJ_OK && r->has_host) {
       host_free(r->host_off, r->host_bytes);
@@ -486,7 +515,24 @@ struct gpj_server {
 
   // Launches the queries of a request whose index is ready, then the copy of
   // its results to the pinned arena.
+  // The queries of a request whose index is ready join this pass's batched
+  // launch (flush_queries); an empty file runs alone (no kernel).
   void launch_queries(Request *r) {
+    Resident *res = r->res;
+    const uint64_t ints = res->lines * r->slots_total * 2u;
+    if (!ensure_results(r, ints)) {
+      r->state = St::WaitMemory;
+      return;
+    }
+    if (res->size == 0 || !group_builds) {
+      launch_queries_alone(r);
+      return;
+    }
+    r->state = St::QueryReady;
+    qready.push_back(r);
+  }
+
+  void launch_queries_alone(Request *r) {
     Resident *res = r->res;
     const uint64_t lines = res->lines;
     const uint64_t ints = lines * r->slots_total * 2u;
@@ -494,6 +540,7 @@ struct gpj_server {
       r->state = St::WaitMemory;
       return;
     }
+    r->status_words = 0;
     Slot &s = slots[r->slot];
     int32_t *d_out = reinterpret_cast<int32_t *>(dptr(r->work_off + r->scratch_bytes));
     cudaError_t e = cudaSuccess;
@@ -798,6 +845,206 @@ struct gpj_server {
     return 1;
   }
 
+  bool query_overflow(const Request *r) const {
+    const unsigned long long *p = slots[r->slot].pinned;
+    unsigned int bits = 0;
+    if (r->status_words == 0) {
+      bits = *reinterpret_cast<const unsigned int *>(p + 7);
+    } else {
+      const auto *w = reinterpret_cast<const unsigned int *>(p + 4);
+      for (uint32_t k = 0; k < r->status_words; ++k) bits |= w[k];
+    }
+    return (bits & gpjb::kQueryStatusOverflow) != 0;
+  }
+
+  // One launch of the multi-file query kernel for every request in qready:
+  // a "file" per (request, query) pair, addressed inside the device arena
+  // (input, bitmaps, newline index, results), with its own status word; then
+  // per request a D2H of its results and status words and its event.
+  void flush_queries() {
+    if (qready.empty()) return;
+    std::vector<Request *> reqs;
+    reqs.swap(qready);
+    // pairs and distinct query IRs (the kernel takes up to kMaxBatchGroups)
+    struct Pair { Request *r; uint32_t q; uint32_t group; };
+    std::vector<Pair> pairs;
+    std::vector<const Request *> group_req;
+    std::vector<uint32_t> group_q;
+    std::vector<Request *> in_batch, alone;
+    uint64_t ir_bytes = 0;
+    for (Request *r : reqs) {
+      std::vector<Pair> mine;
+      bool fits = true;
+      uint64_t added_ir = 0;
+      std::vector<std::pair<const Request *, uint32_t>> new_groups;
+      for (uint32_t q = 0; q < r->queries.size(); ++q) {
+        const gpj_batch_query &bq = r->queries[q];
+        uint32_t g = 0;
+        bool found = false;
+        for (; g < group_req.size(); ++g) {
+          const gpj_batch_query &o = group_req[g]->queries[group_q[g]];
+          if (o.num_result_slots == bq.num_result_slots && o.base_level == bq.base_level &&
+              group_req[g]->irs[group_q[g]] == r->irs[q]) {
+            found = true;
+            break;
+          }
+        }
+        if (!found) {
+          for (size_t k = 0; k < new_groups.size(); ++k) {
+            const Request *nr = new_groups[k].first;
+            const uint32_t nq = new_groups[k].second;
+            if (nr->queries[nq].num_result_slots == bq.num_result_slots &&
+                nr->queries[nq].base_level == bq.base_level && nr->irs[nq] == r->irs[q]) {
+              g = uint32_t(group_req.size() + k);
+              found = true;
+              break;
+            }
+          }
+        }
+        if (!found) {
+          g = uint32_t(group_req.size() + new_groups.size());
+          new_groups.emplace_back(r, q);
+          added_ir += r->irs[q].size();
+        }
+        mine.push_back(Pair{r, q, g});
+      }
+      if (group_req.size() + new_groups.size() > size_t(gpjb::kMaxBatchGroups) ||
+          ir_bytes + added_ir > uint64_t(gpjb::kMaxQueryIrBytes))
+        fits = false;
+      if (!fits) {
+        alone.push_back(r);
+        continue;
+      }
+      for (auto &ng : new_groups) {
+        group_req.push_back(ng.first);
+        group_q.push_back(ng.second);
+      }
+      ir_bytes += added_ir;
+      pairs.insert(pairs.end(), mine.begin(), mine.end());
+      in_batch.push_back(r);
+    }
+    for (Request *r : alone) launch_queries_alone(r);
+    if (in_batch.empty()) return;
+    const uint64_t V = pairs.size();
+    const uint64_t files_bytes = align_up(V * sizeof(gpjb::IndexFile));
+    const uint64_t rows_bytes = align_up(V * 64u + 32u);
+    const uint64_t meta_bytes = files_bytes + rows_bytes + align_up(V * 4u);
+    const uint64_t host_bytes = files_bytes + rows_bytes;
+    auto owned = std::make_unique<QBatch>();
+    QBatch *b = owned.get();
+    bool ok = dev_alloc(meta_bytes, &b->meta_off);
+    if (ok) b->meta_bytes = block_size(meta_bytes);
+    ok = ok && host_alloc(host_bytes, &b->host_off);
+    if (ok) b->host_bytes = block_size(host_bytes);
+    if (!ok) {
+      if (b->meta_bytes) dev_free(b->meta_off, b->meta_bytes);
+      for (Request *r : in_batch) launch_queries_alone(r);
+      return;
+    }
+    auto *h_files = reinterpret_cast<gpjb::IndexFile *>(
+        reinterpret_cast<uint8_t *>(h_arena) + b->host_off);
+    auto *h_rows = reinterpret_cast<uint64_t *>(
+        reinterpret_cast<uint8_t *>(h_arena) + b->host_off + files_bytes);
+    auto *d_files = reinterpret_cast<gpjb::IndexFile *>(dptr(b->meta_off));
+    auto *d_rows = reinterpret_cast<uint64_t *>(dptr(b->meta_off + files_bytes));
+    auto *d_stat = reinterpret_cast<unsigned int *>(dptr(b->meta_off + files_bytes + rows_bytes));
+    uint64_t records = 0;
+    for (uint64_t v = 0; v < V; ++v) {
+      const Pair &pr = pairs[v];
+      Request *r = pr.r;
+      const Resident *res = r->res;
+      const gpj_batch_query &bq = r->queries[pr.q];
+      uint64_t off = 0;
+      for (uint32_t q = 0; q < pr.q; ++q) off += res->lines * r->queries[q].num_result_slots * 2u;
+      r->resp.result_offset[pr.q] = off;
+      gpjb::IndexFile F;
+      F.in_off = uint64_t(res->d_input - d_arena);
+      F.n = res->size;
+      F.s_off = uint64_t(reinterpret_cast<uint8_t *>(res->S) - d_arena) / 8u;
+      F.lb_off = uint64_t(reinterpret_cast<uint8_t *>(res->LB) - d_arena) / 8u;
+      F.first_tile = 0;
+      F.levels = res->levels;
+      h_files[v] = F;
+      uint64_t *row = h_rows + v * 8u;
+      const uint64_t out_int = (r->work_off + r->scratch_bytes) / 4u + off;
+      row[gpjb::kFiLines] = res->lines;
+      row[gpjb::kFiNlOff] = uint64_t(reinterpret_cast<uint8_t *>(res->NL) - d_arena) / 8u;
+      row[gpjb::kFiRecOff] = records;
+      row[gpjb::kFiOutOff] = out_int;
+      row[gpjb::kFiInString] = 0;
+      row[gpjb::kFiDepth] = 0;
+      row[gpjb::kFiBytes] = res->size;
+      row[gpjb::kFiQuery] = pr.group;
+      records += bq.num_result_slots > 0 ? res->lines : 0u;
+      if (bq.num_result_slots == 0) row[gpjb::kFiLines] = 0;
+    }
+    uint64_t *h_tot = h_rows + V * 8u;
+    h_tot[gpjb::kTotRecords] = records;
+    h_tot[gpjb::kTotResultInts] = 0;
+    h_tot[gpjb::kTotNlSlots] = 0;
+    h_tot[gpjb::kTotError] = 0;
+    gpjb::BatchQueryLaunch ql;
+    ql.in = d_arena;
+    ql.S = reinterpret_cast<const uint64_t *>(d_arena);
+    ql.LB = reinterpret_cast<const uint64_t *>(d_arena);
+    ql.NL = reinterpret_cast<const int64_t *>(d_arena);
+    ql.files = d_files;
+    ql.num_files = uint32_t(V);
+    ql.file_info = d_rows;
+    ql.totals = d_rows + V * 8u;
+    ql.out = reinterpret_cast<int32_t *>(d_arena);
+    ql.file_status = d_stat;
+    ql.num_groups = int(group_req.size());
+    gpjb::IrBlob blob;
+    std::memset(blob.bytes, 0, sizeof(blob.bytes));
+    int ir_off = 0;
+    for (size_t g = 0; g < group_req.size(); ++g) {
+      const Request *gr = group_req[g];
+      const uint32_t gq = group_q[g];
+      std::memcpy(blob.bytes + ir_off, gr->irs[gq].data(), gr->irs[gq].size());
+      ql.groups[g].ir_off = ir_off;
+      ql.groups[g].ir_len = int(gr->irs[gq].size());
+      ql.groups[g].num_results = int(gr->queries[gq].num_result_slots);
+      ql.groups[g].base_level = int(gr->queries[gq].base_level);
+      ir_off += int(gr->irs[gq].size());
+    }
+    Slot &s0 = slots[in_batch[0]->slot];
+    cudaError_t e = cudaMemcpyAsync(d_files, h_files, files_bytes + V * 64u + 32u,
+                                    cudaMemcpyHostToDevice, s0.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_stat, 0, V * 4u, s0.stream);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg.device);
+    const uint64_t blocks = (records + 127u) / 128u;
+    const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(blocks, uint64_t(sms) * 8u)));
+    if (e == cudaSuccess && records > 0) e = gpjb::batch_query_launch(ql, blob, grid, 128, s0.stream);
+    b->refs = int(in_batch.size());
+    qbatches.emplace(b, std::move(owned));
+    uint64_t v = 0;
+    for (Request *r : in_batch) {
+      Slot &s = slots[r->slot];
+      const uint64_t ints = r->res->lines * r->slots_total * 2u;
+      const uint32_t nq = uint32_t(r->queries.size());
+      r->qbatch = b;
+      r->status_words = nq;
+      if (e == cudaSuccess && ints > 0)
+        e = cudaMemcpyAsync(h_arena + r->host_off / 4u, dptr(r->work_off + r->scratch_bytes),
+                            ints * 4u, cudaMemcpyDeviceToHost, s0.stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(reinterpret_cast<unsigned int *>(s.pinned + 4), d_stat + v, nq * 4u,
+                            cudaMemcpyDeviceToHost, s0.stream);
+      if (e == cudaSuccess) e = cudaEventRecord(s.event, s0.stream);
+      v += nq;
+      r->resp.num_lines = r->res->lines;
+      r->resp.result_ints = ints;
+      r->state = St::Querying;
+    }
+    if (e != cudaSuccess) {
+      const std::string msg = std::string("batched query: ") + cudaGetErrorString(e);
+      const int code = cuda_status(e);
+      for (Request *r : in_batch) finish(r, code, msg);
+    }
+  }
+
   bool advance() {
     bool any = false;
     const std::vector<Request *> snap(active);
@@ -812,8 +1059,7 @@ struct gpj_server {
           else finish(r, cuda_status(e), msg);
         } else if (r->state == St::Indexing) {
           on_index_done(r);
-        } else if (*reinterpret_cast<const unsigned int *>(slots[r->slot].pinned + 7) &
-                   gpjb::kQueryStatusOverflow) {
+        } else if (query_overflow(r)) {
           finish(r, GPJ_ERR_CAPACITY,
                  "a record has more results than result slots; the results are truncated");
         } else {
@@ -1023,6 +1269,7 @@ struct gpj_server {
       }
       bool progressed = advance();
       progressed = admit() || progressed;
+      flush_queries();
       std::unique_lock<std::mutex> lk(mu);
       stats.in_flight = active.size();
       stats.pending = pending.size();

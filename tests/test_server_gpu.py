@@ -222,3 +222,26 @@ def test_grouped_builds_equal_single_builds(gpj):
                 np.testing.assert_array_equal(grouped[i].results[0].astype(np.int64),
                                               _oracle(data, c, base, lv), err_msg=f"file {fi}")
                 break
+
+
+def test_overflow_status_per_request(gpj):
+    """In a batched query launch each (request, query) pair has its own
+    status word: only the request whose "[*]" array outgrows its limit fails
+    (GPJ_ERR_CAPACITY); the others in the same pass succeed."""
+    _need_gpu()
+    from gpjson_b200 import datagen
+    data = np.array(datagen.tweets(12, 1 << 20))
+    short = gpj.compile("$.entities.hashtags[*].text", wildcard_limit=2)
+    full = gpj.compile("$.entities.hashtags[*].text", wildcard_limit=8)
+    lang = gpj.compile("$.user.lang")
+    with gpj.Server(num_slots=8, hbm_budget_bytes=256 << 20) as s:
+        ids = [s.submit(data, [(full, 0, 3)], file_key=1),
+               s.submit(data, [(lang, 0, 3), (short, 0, 3)], file_key=1),
+               s.submit(data, [(lang, 0, 3)], file_key=1)]
+        for rid in ids:
+            s.wait(rid)
+        rs = [s.response(rid) for rid in ids]
+    assert rs[0].status == 0 and rs[2].status == 0
+    assert rs[1].status == gpj.GPJ_ERR_CAPACITY and "result slots" in rs[1].message
+    np.testing.assert_array_equal(rs[0].results[0].astype(np.int64), _oracle(data, full, 0, 3))
+    np.testing.assert_array_equal(rs[2].results[0].astype(np.int64), _oracle(data, lang, 0, 3))
