@@ -585,7 +585,10 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(data, comp, records, levels, budget_s=12.0)
+        got = [o.cpu().numpy().astype(np.int64).reshape(lines, c.num_result_slots, 2)
+               for (c, _), o in zip(comp, outs)]
+        line["cpu_baseline"], line["parity"] = cpu_baseline(data, comp, records, levels,
+                                                            budget_s=12.0, results=got)
     if rank == 0 and args.ref_gpu:
         line["reference_gpu"] = reference_gpu(data, queries, records, levels, ms_index,
                                               ms_step - ms_index)
@@ -922,9 +925,13 @@ def _partitions(data: np.ndarray, parts: int):
     return [(a, b) for a, b in zip(bounds, bounds[1:]) if b > a]
 
 
-def cpu_baseline(data, comp, records, levels, budget_s: float, threads: int | None = None):
+def cpu_baseline(data, comp, records, levels, budget_s: float, threads: int | None = None,
+                 results=None):
     """Times the oracle (the reference algorithm restated in C) on a bounded,
-    newline-aligned sample with one partition per host thread."""
+    newline-aligned sample with one partition per host thread.  With
+    `results` (this engine's per-query result arrays for the whole input,
+    partition offsets) the oracle's results of the sample are compared with
+    them: returns (baseline, parity)."""
     import oracle
     threads = threads or os.cpu_count() or 1
     sample = min(data.size, 96 << 20)
@@ -933,21 +940,36 @@ def cpu_baseline(data, comp, records, levels, budget_s: float, threads: int | No
     def work(ab):
         a, b = ab
         ix = oracle.OracleIndex(data[a:b], levels)
-        for c, base in comp:
-            # a partition cut out of a top-level array holds its elements at
-            # depth 0, except the first one, which holds the opening bracket
-            ix.query(c.ir_bytes, c.num_result_slots, base if a == 0 else 0)
-        return b - a
+        # a partition cut out of a top-level array holds its elements at
+        # depth 0, except the first one, which holds the opening bracket
+        return [ix.query(c.ir_bytes, c.num_result_slots, base if a == 0 else 0)
+                for c, base in comp]
 
     t0 = time.perf_counter()
-    done = 0
     with cf.ThreadPoolExecutor(threads) as pool:
-        for got in pool.map(work, parts):
-            done += got
+        got = list(pool.map(work, parts))
     dt = time.perf_counter() - t0
-    return {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
+    done = sum(b - a for a, b in parts)
+    base = {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
             "kind": "port", "sample": f"first {done} bytes of the workload, "
             f"{len(parts)} newline-aligned partitions, {threads} threads"}
+    if results is None:
+        return base
+    # partition k starts after a newline; its lines are the input's lines
+    # from (newlines before it) on, and its last line (after the newline that
+    # ends it) is empty unless it is the last partition of the input
+    checked = 0
+    for (a, b), per_query in zip(parts, got):
+        first = int(np.count_nonzero(data[:a] == 10))
+        for q, want in enumerate(per_query):
+            w = want if b == data.size else want[:-1]
+            w = np.where(w >= 0, w + a, w)
+            g = np.asarray(results[q][first:first + w.shape[0]]).astype(np.int64)
+            if g.shape != w.shape or not np.array_equal(g, w):
+                raise AssertionError(f"parity: query {q} differs from the oracle in [{a}, {b})")
+            checked += w.shape[0]
+    return base, {"oracle": "oracle/gpjson_oracle.c on newline partitions of the first "
+                            f"{done} bytes", "records_checked": checked, "mismatches": 0}
 
 
 def run_reference(args, world, rank):

@@ -55,3 +55,25 @@ def test_c3_sizes_match_the_spec():
     assert sizes.size == 10_000
     assert sizes.min() >= 4 << 10 and sizes.max() <= 64 << 20
     assert abs(int(sizes.sum()) - (8 << 30)) < (64 << 20)
+
+
+def test_cpu_baseline_parity_gate(gpj):
+    """The single-input lines' parity gate: the oracle's results on the
+    sample's newline partitions, shifted, equal the whole-input results, and a
+    planted difference fails the line."""
+    import oracle
+    from gpjson_b200 import datagen
+    data = datagen.tweets(5, 3 << 20)
+    comp = bench.compile_all(gpj, ["$.user.lang", "$.entities.hashtags[*].text"])
+    levels = max(c.max_depth + b for c, b in comp)
+    ix = oracle.OracleIndex(data, levels)
+    whole = [ix.query(c.ir_bytes, c.num_result_slots, b) for c, b in comp]
+    base, parity = bench.cpu_baseline(data, comp, "lines", levels, 1.0, threads=3,
+                                      results=whole)
+    assert parity["mismatches"] == 0 and parity["records_checked"] >= 2 * (ix.num_lines - 1)
+    bad = [w.copy() for w in whole]
+    hit = np.argwhere(bad[0][:, 0, 0] >= 0).ravel()
+    bad[0][hit[len(hit) // 2], 0, 1] += 1
+    import pytest
+    with pytest.raises(AssertionError, match="parity"):
+        bench.cpu_baseline(data, comp, "lines", levels, 1.0, threads=3, results=bad)
