@@ -350,7 +350,7 @@ int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
       b->index_threads = threads;
       if ((rc = alloc_layout_buffers(b)) != GPJ_OK) return bail(rc);
       for (int block : {128, 256}) {
-        for (int gm : {4, 8, 16}) {
+        for (int gm : {4, 5, 8, 16}) {
           b->query_block = block;
           b->query_grid = sms * gm * (256 / block);
           const float ms = time_chain(b, s, 3);

@@ -687,56 +687,55 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
   st.nl_ex = nl_ex;
 }
 
-// Leveled bitmaps of one lane's two words, walked as one event sequence
-// (word 0, then word 1 with the depth carried over), so a warp iterates as
-// often as its busiest lane has events in both words together.  Separators
+// Leveled bitmaps of one lane's two words, walked as one event sequence in
+// 32-bit quarters (word 0 low, word 0 high, word 1 low, word 1 high, the
+// depth carried over), so every step is 32-bit integer work and a warp
+// iterates as often as its busiest lane has events in its row.  Separators
 // between two events share one depth; an opening bracket belongs to the
 // level it opens, a closing one to the level it closes (signed-char depth,
 // sharemem/leveled-bitmaps-index.cu:270-300).  Each mask is OR-ed into the
-// lane's own shared-memory slot of its level.
+// lane's own shared-memory slot of its level and quarter.
 template <int LMAX, int NT>
 __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_t O0,
                                              uint64_t C0, uint64_t P0, uint64_t O1, uint64_t C1,
                                              uint64_t P1, int depth0, uint64_t (&lb0)[LMAX],
                                              uint64_t (&lb1)[LMAX]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint64_t *slot = &ls.lb[warp][0][2 * lane];  // [level * 64 + word]
+  uint64_t *slot64 = &ls.lb[warp][0][2 * lane];  // [level * 64 + word]
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
-    slot[l * 64] = 0ull;
-    slot[l * 64 + 1] = 0ull;
+    slot64[l * 64] = 0ull;
+    slot64[l * 64 + 1] = 0ull;
   }
-  uint64_t O = O0, Pm = P0, ev = O0 | C0, acc = 0, done = 0;
-  int h = 0, d = depth0;
-  for (;;) {
-    if (ev == 0) {
-      // separators after the word's last event
-      const uint64_t m = acc | (Pm & ~done);
-      if (m != 0 && d >= 0 && d < LMAX) slot[d * 64 + h] |= m;
-      if (h == 1) break;
-      h = 1;
-      O = O1;
-      Pm = P1;
-      ev = O1 | C1;
-      acc = 0;
-      done = 0;
-      continue;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(slot64);  // [level * 128 + quarter]
+  int d = depth0;
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const uint64_t Ow = h < 2 ? O0 : O1, Cw = h < 2 ? C0 : C1, Pw = h < 2 ? P0 : P1;
+    const uint32_t O = uint32_t((h & 1) ? (Ow >> 32) : Ow);
+    const uint32_t C = uint32_t((h & 1) ? (Cw >> 32) : Cw);
+    const uint32_t Pm = uint32_t((h & 1) ? (Pw >> 32) : Pw);
+    uint32_t ev = O | C, acc = 0u, done = 0u;
+    while (ev) {  // branch-free body: lanes only differ in the trip count
+      const uint32_t bit = ev & (0u - ev);
+      const uint32_t below = bit - 1u;
+      acc |= Pm & below & ~done;
+      const bool open = (O & bit) != 0u;
+      const uint32_t m = acc | (bit & ~O);  // a closing bracket joins its level
+      if (m != 0u && unsigned(d) < unsigned(LMAX)) slot[d * 128 + h] |= m;
+      d = int(int8_t(uint8_t(open ? d + 1 : d - 1)));
+      acc = open ? bit : 0u;
+      done = below | bit;
+      ev &= ev - 1u;
     }
-    const uint64_t bit = ev & (0 - ev);
-    const uint64_t below = bit - 1;
-    acc |= Pm & below & ~done;
-    const bool open = (O & bit) != 0;
-    const uint64_t m = open ? acc : (acc | bit);
-    if (m != 0 && d >= 0 && d < LMAX) slot[d * 64 + h] |= m;
-    d = int(int8_t(uint8_t(open ? d + 1 : d - 1)));
-    acc = open ? bit : 0ull;
-    done = below | bit;
-    ev &= ev - 1;
+    // separators after the quarter's last event
+    const uint32_t m = acc | (Pm & ~done);
+    if (m != 0u && unsigned(d) < unsigned(LMAX)) slot[d * 128 + h] |= m;
   }
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
-    lb0[l] = slot[l * 64];
-    lb1[l] = slot[l * 64 + 1];
+    lb0[l] = slot64[l * 64];
+    lb1[l] = slot64[l * 64 + 1];
   }
 }
 

@@ -205,19 +205,24 @@ def test_grouped_builds_equal_single_builds(gpj):
 
     grouped, st_g = run(0)
     alone, st_a = run(gpj.GPJ_SERVER_NO_GROUPS)
-    assert st_g["failed"] == 0 and st_a["failed"] == 0
     assert st_g["index_launches"] < st_g["cache_misses"], st_g
     assert st_a["index_launches"] >= st_a["cache_misses"] - 2, st_a  # empty files launch nothing
     assert st_g["rebuilds"] >= 1
+    assert st_g["failed"] == st_a["failed"]
     for i, (key, data, qs, names) in enumerate(reqs):
         g, a = grouped[i], alone[i]
-        assert g.status == 0 and a.status == 0, (g.message, a.message)
+        # the random-structure file can hold an array longer than the "[*]"
+        # limit: that request fails with the same status in both modes
+        assert g.status == a.status, (i, g.message, a.message)
+        assert g.status in (0, gpj.GPJ_ERR_CAPACITY), g.message
+        if g.status:
+            continue
         assert g.num_lines == a.num_lines
         for (c, base, lv), qg, qa in zip(qs, g.results, a.results):
             np.testing.assert_array_equal(qg, qa, err_msg=f"request {i}")
     for fi, (kind, data) in enumerate(files):
         for i, (key, d, qs, names) in enumerate(reqs):
-            if key == fi + 1:
+            if key == fi + 1 and grouped[i].status == 0:
                 c, base, lv = qs[0]
                 np.testing.assert_array_equal(grouped[i].results[0].astype(np.int64),
                                               _oracle(data, c, base, lv), err_msg=f"file {fi}")
@@ -234,14 +239,15 @@ def test_overflow_status_per_request(gpj):
     short = gpj.compile("$.entities.hashtags[*].text", wildcard_limit=2)
     full = gpj.compile("$.entities.hashtags[*].text", wildcard_limit=8)
     lang = gpj.compile("$.user.lang")
+    L = full.max_depth
     with gpj.Server(num_slots=8, hbm_budget_bytes=256 << 20) as s:
-        ids = [s.submit(data, [(full, 0, 3)], file_key=1),
-               s.submit(data, [(lang, 0, 3), (short, 0, 3)], file_key=1),
-               s.submit(data, [(lang, 0, 3)], file_key=1)]
+        ids = [s.submit(data, [(full, 0, L)], file_key=1),
+               s.submit(data, [(lang, 0, L), (short, 0, L)], file_key=1),
+               s.submit(data, [(lang, 0, L)], file_key=1)]
         for rid in ids:
             s.wait(rid)
         rs = [s.response(rid) for rid in ids]
     assert rs[0].status == 0 and rs[2].status == 0
     assert rs[1].status == gpj.GPJ_ERR_CAPACITY and "result slots" in rs[1].message
-    np.testing.assert_array_equal(rs[0].results[0].astype(np.int64), _oracle(data, full, 0, 3))
-    np.testing.assert_array_equal(rs[2].results[0].astype(np.int64), _oracle(data, lang, 0, 3))
+    np.testing.assert_array_equal(rs[0].results[0].astype(np.int64), _oracle(data, full, 0, L))
+    np.testing.assert_array_equal(rs[2].results[0].astype(np.int64), _oracle(data, lang, 0, L))
