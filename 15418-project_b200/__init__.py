@@ -55,7 +55,8 @@ EXPORTED_SYMBOLS = (
     "gpj_batch_create", "gpj_batch_run", "gpj_batch_run_stages", "gpj_batch_run_per_file",
     "gpj_batch_run_host",
     "gpj_batch_view_get", "gpj_batch_file_layout", "gpj_batch_destroy",
-    "gpj_server_create", "gpj_server_submit", "gpj_server_poll", "gpj_server_wait",
+    "gpj_server_create", "gpj_server_submit", "gpj_server_submit_many", "gpj_server_poll",
+    "gpj_server_wait",
     "gpj_server_response", "gpj_server_release", "gpj_server_stats_get",
     "gpj_server_clear_cache", "gpj_server_destroy",
 )
@@ -251,6 +252,7 @@ def load_library(build_if_missing: bool = False) -> C.CDLL:
     lib.gpj_batch_destroy.argtypes = [vp]
     lib.gpj_server_create.argtypes = [P(ServerConfig), P(vp)]
     lib.gpj_server_submit.argtypes = [vp, P(Request), P(u64)]
+    lib.gpj_server_submit_many.argtypes = [vp, vp, u32, vp]
     lib.gpj_server_poll.argtypes = [vp, P(u64), u32, P(u32), C.c_int64]
     lib.gpj_server_wait.argtypes = [vp, u64, C.c_int64]
     lib.gpj_server_response.argtypes = [vp, u64, P(Response)]
@@ -585,6 +587,33 @@ class Server:
         _check(self._lib.gpj_server_submit(self._h, C.byref(req), C.byref(rid)))
         self._keep[rid.value] = (arr, [c.num_result_slots for c, _, _ in queries])
         return rid.value
+
+    def prepare(self, items):
+        """Builds the request table of gpj_server_submit_many for a list of
+        (data, queries, file_key, arrival_ns) items; submit_prepared queues it
+        with one call."""
+        import numpy as np
+        reqs = (Request * max(1, len(items)))()
+        keep = []
+        for i, (data, queries, key, arrival) in enumerate(items):
+            arr = np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data
+            irs = [(C.c_uint8 * max(1, len(c.ir_bytes))).from_buffer_copy(c.ir_bytes or b"\0")
+                   for c, _, _ in queries]
+            qa = (BatchQuery * len(queries))(*[
+                BatchQuery(C.addressof(ir), len(c.ir_bytes), c.num_result_slots, base, lv, 0)
+                for (c, base, lv), ir in zip(queries, irs)])
+            reqs[i] = Request(key, arr.ctypes.data if arr.size else None, arr.size,
+                              C.cast(qa, C.c_void_p), len(queries), 0, arrival)
+            keep.append((arr, [c.num_result_slots for c, _, _ in queries], irs, qa))
+        return reqs, keep
+
+    def submit_prepared(self, prepared) -> list:
+        reqs, keep = prepared
+        ids = (C.c_uint64 * max(1, len(keep)))()
+        _check(self._lib.gpj_server_submit_many(self._h, C.cast(reqs, C.c_void_p), len(keep), ids))
+        for rid, (arr, slots, _, _) in zip(ids[:len(keep)], keep):
+            self._keep[rid] = (arr, slots)
+        return list(ids[:len(keep)])
 
     def poll(self, capacity: int = 1024, timeout_us: int = 0) -> list:
         ids = (C.c_uint64 * capacity)()

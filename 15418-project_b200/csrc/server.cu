@@ -1398,9 +1398,9 @@ int gpj_server_create(const gpj_server_config *config, gpj_server **out) {
   return GPJ_OK;
 }
 
-int gpj_server_submit(gpj_server *s, const gpj_request *req, uint64_t *request_id) {
-  if (s == nullptr || req == nullptr || request_id == nullptr)
-    return fail(GPJ_ERR_INVALID_ARGUMENT, "gpj_server_submit: null argument");
+namespace {
+// Checks one request and copies it (and its IRs) into a new Request.
+int make_request(const gpj_request *req, std::unique_ptr<Request> *out) {
   if (req->num_queries == 0 || req->num_queries > GPJ_SERVER_MAX_QUERIES || req->queries == nullptr)
     return fail(GPJ_ERR_INVALID_ARGUMENT, "gpj_server_submit: 1 to 8 queries per request");
   if (req->size_bytes > 0x7FFFFFFFull)
@@ -1429,15 +1429,38 @@ int gpj_server_submit(gpj_server *s, const gpj_request *req, uint64_t *request_i
     r->slots_total += bq.num_result_slots;
   }
   r->resp.arrival_ns = req->arrival_ns ? req->arrival_ns : now_ns();
+  *out = std::move(r);
+  return GPJ_OK;
+}
+}  // namespace
+
+int gpj_server_submit_many(gpj_server *s, const gpj_request *reqs, uint32_t count,
+                           uint64_t *request_ids) {
+  if (s == nullptr || (count > 0 && (reqs == nullptr || request_ids == nullptr)))
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "gpj_server_submit_many: null argument");
+  std::vector<std::unique_ptr<Request>> made(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    const int rc = make_request(&reqs[i], &made[i]);
+    if (rc != GPJ_OK) return rc;  // nothing was queued
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return fail(GPJ_ERR_EXECUTION, "gpj_server_submit: server is shutting down");
-  r->id = s->next_id++;
-  *request_id = r->id;
-  s->pending.push_back(r.get());
-  s->requests.emplace(r->id, std::move(r));
-  s->stats.submitted++;
+  for (uint32_t i = 0; i < count; ++i) {
+    Request *r = made[i].get();
+    r->id = s->next_id++;
+    request_ids[i] = r->id;
+    s->pending.push_back(r);
+    s->requests.emplace(r->id, std::move(made[i]));
+  }
+  s->stats.submitted += count;
   s->cv_sched.notify_one();
   return GPJ_OK;
+}
+
+int gpj_server_submit(gpj_server *s, const gpj_request *req, uint64_t *request_id) {
+  if (s == nullptr || req == nullptr || request_id == nullptr)
+    return fail(GPJ_ERR_INVALID_ARGUMENT, "gpj_server_submit: null argument");
+  return gpj_server_submit_many(s, req, 1, request_id);
 }
 
 int gpj_server_poll(gpj_server *s, uint64_t *ids, uint32_t capacity, uint32_t *count,

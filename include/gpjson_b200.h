@@ -453,6 +453,12 @@ int gpj_server_create(const gpj_server_config *config, gpj_server **out);
 /* Queues a request (copies the request and its IRs); returns its id. */
 int gpj_server_submit(gpj_server *server, const gpj_request *request, uint64_t *request_id);
 
+/* Queues `count` requests at once (one lock, one wake-up of the scheduler);
+ * request_ids[i] gets the id of requests[i].  All are checked first: on an
+ * error nothing is queued. */
+int gpj_server_submit_many(gpj_server *server, const gpj_request *requests, uint32_t count,
+                           uint64_t *request_ids);
+
 /* Waits up to timeout_us (negative: forever) for finished requests not yet
  * reported by this call and returns up to capacity of their ids. */
 int gpj_server_poll(gpj_server *server, uint64_t *ids, uint32_t capacity, uint32_t *count,

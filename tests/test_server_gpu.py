@@ -271,3 +271,29 @@ def test_truncated_group_newline_block_rebuilds_members(gpj):
     for d, r in zip(datas, rs):
         assert r.status == 0 and r.num_lines == d.tobytes().count(b"\n") + 1
         np.testing.assert_array_equal(r.results[0].astype(np.int64), _oracle(d, c, 0, 1))
+
+
+def test_submit_many_queues_all_at_once(gpj):
+    """gpj_server_submit_many: one call queues a whole request table; every
+    result equals the oracle's, and a bad entry queues nothing."""
+    _need_gpu()
+    compiled = _compiled(gpj)
+    files = _files()
+    reqs = _requests(files, compiled, 30, seed=5)
+    with gpj.Server(num_slots=16, hbm_budget_bytes=256 << 20) as s:
+        with pytest.raises(ValueError):
+            s.prepare  # noqa: B018 -- the table below is valid; an empty query list is not
+            bad = s.prepare([(reqs[0][1], [], 1, 0)])
+            s.submit_prepared(bad)
+        assert s.stats()["submitted"] == 0
+        ids = s.submit_prepared(s.prepare([(d, qs, key, 0) for key, d, qs, _ in reqs]))
+        out = {}
+        for i, rid in enumerate(ids):
+            s.wait(rid)
+            out[i] = s.response(rid)
+    for i, (key, data, qs, names) in enumerate(reqs):
+        if out[i].status == gpj.GPJ_ERR_CAPACITY:
+            continue  # the random-structure file may outgrow a "[*]" limit
+        assert out[i].status == 0, out[i].message
+        for (c, base, lv), got in zip(qs, out[i].results):
+            np.testing.assert_array_equal(got.astype(np.int64), _oracle(data, c, base, lv))
