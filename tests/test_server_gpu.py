@@ -281,10 +281,8 @@ def test_submit_many_queues_all_at_once(gpj):
     files = _files()
     reqs = _requests(files, compiled, 30, seed=5)
     with gpj.Server(num_slots=16, hbm_budget_bytes=256 << 20) as s:
-        with pytest.raises(ValueError):
-            s.prepare  # noqa: B018 -- the table below is valid; an empty query list is not
-            bad = s.prepare([(reqs[0][1], [], 1, 0)])
-            s.submit_prepared(bad)
+        with pytest.raises(ValueError):  # a request without queries
+            s.submit_prepared(s.prepare([(reqs[0][1], [], 1, 0)]))
         assert s.stats()["submitted"] == 0
         ids = s.submit_prepared(s.prepare([(d, qs, key, 0) for key, d, qs, _ in reqs]))
         out = {}
