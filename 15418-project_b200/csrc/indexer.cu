@@ -591,8 +591,9 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
   const uint64_t Q1 = c1.qt & ~E1;
   const uint64_t Sl0 = prefix_xor(Q0);
   const uint64_t Sl1 = prefix_xor(Q1);
-  const uint32_t par0 = uint32_t(popc64(Q0)) & 1u;
-  const uint32_t par1 = uint32_t(popc64(Q1)) & 1u;
+  // a word's quote parity is the top bit of its in-word prefix-XOR
+  const uint32_t par0 = uint32_t(Sl0 >> 63);
+  const uint32_t par1 = uint32_t(Sl1 >> 63);
   if (P.E != nullptr) {
     const uint64_t W = (F.n + 63u) / 64u;
     store2(P.E + F.s_off, lw0, W, E0 & valid_mask(lw0, F.n), E1 & valid_mask(lw0 + 1, F.n));
