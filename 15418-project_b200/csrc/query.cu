@@ -127,16 +127,51 @@ __device__ Pos next_struct(const Rec<Pos> &c, WordCache<Pos> &wc, Pos level_end,
   if (line_index >= level_end || lvl == nullptr) return level_end;
   Pos wi = line_index >> 6;
   Pos base = wi * 64;
-  uint64_t word = cached_word(wc, lvl, c.W, wi) & (~0ull << (line_index - base));
-  while (base <= level_end) {
-    uint64_t cand = word;
+  {
+    uint64_t cand = cached_word(wc, lvl, c.W, wi) & (~0ull << (line_index - base));
     const Pos last = level_end - base;
     if (last < 63) cand &= mask_through_bit(int(last));
     if (cand != 0) return base + __ffsll(static_cast<long long>(cand)) - 1;
+  }
+  // A long gap (a string value, a skipped member) spans several words: scan
+  // them two at a time with one 16-byte load per aligned pair.  Words past W
+  // are zero, so the scan may stop there.
+  ++wi;
+  base += 64;
+  while (base <= level_end && wi < c.W) {
+    const bool pair = ((reinterpret_cast<uintptr_t>(lvl + wi) & 15u) == 0) && wi + 1 < c.W;
+    uint64_t w0, w1 = 0ull;
+    if (pair) {
+      const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(lvl + wi);
+      w0 = v.x;
+      w1 = v.y;
+    } else {
+      w0 = lvl[wi];
+    }
+    uint64_t cand = w0;
+    Pos last = level_end - base;
+    if (last < 63) cand &= mask_through_bit(int(last));
+    if (cand != 0) {
+      wc.bm = lvl;
+      wc.idx = wi;
+      wc.val = w0;
+      return base + __ffsll(static_cast<long long>(cand)) - 1;
+    }
     ++wi;
     base += 64;
+    if (!pair) continue;
     if (base > level_end) break;
-    word = cached_word(wc, lvl, c.W, wi);
+    cand = w1;
+    last = level_end - base;
+    if (last < 63) cand &= mask_through_bit(int(last));
+    if (cand != 0) {
+      wc.bm = lvl;
+      wc.idx = wi;
+      wc.val = w1;
+      return base + __ffsll(static_cast<long long>(cand)) - 1;
+    }
+    ++wi;
+    base += 64;
   }
   return level_end;
 }
