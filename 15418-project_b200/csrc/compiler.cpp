@@ -7,15 +7,22 @@
 // (query_compiler.cpp:20-26) and counting result slots and levels the same
 // way.  Queries in the reference's syntax compile to the reference's IR byte
 // for byte.  Extensions (the reference rejects all of them):
-//  * "[*]" with a wildcard limit K > 0: an element-count check (opcode 0x0C,
-//    raises the overflow status when the array holds more than K elements)
-//    followed by exactly the IR of "[0:K]" (query_compiler.cpp:287-289);
+//  * "[*]" with a wildcard limit K > 0: the open slice "[0:]" below (the
+//    reference rejects "[*]", query_compiler.cpp:287-289);
 //  * "..name" as the last step, with a wildcard limit K > 0: every member
 //    named `name` inside the current value at any indexed level, in document
 //    order, into K result slots (opcode 0x0B; query_compiler.cpp:202-204);
 //  * numeric filters "[?(@<path> <op> <number>)]" with op one of == != < <=
 //    > >= (opcode 0x0A: exact decimal comparison), and "!=" ... the filter
-//    of the reference takes only == "string" (query_compiler.cpp:366-391).
+//    of the reference takes only == "string" (query_compiler.cpp:366-391);
+//  * slices counted from the end: "[-a:-b]" (the reverse indexes a .. b+1,
+//    reference IR only), and, with a wildcard limit K > 0, the open slices
+//    "[a:]", "[a:-b]" and "[:-b]": an element-count check (opcode 0x0C,
+//    raises the overflow status when the slice holds more than K elements)
+//    and K forward branches as in "[a:a+K]", each checking that its element
+//    exists and is followed by b more (opcode 0x0D; an empty array has no
+//    element 0, where "[0]" of the reference stores the closing bracket).  The reference parses "[-a:" only
+//    as "[-a:]" and rejects the others (query_compiler.cpp:256-286).
 #include "compiler.hpp"
 
 #include <algorithm>
@@ -39,6 +46,7 @@ enum Op : uint8_t {
   kNumberCompare = 10,  // extension: cmp byte, varint length, number text
   kDescendKey = 11,     // extension: varint length, key bytes
   kExpectAtMost = 12,   // extension: varint element limit
+  kExpectFollowing = 13,  // extension: varint count of elements that must follow
 };
 
 // Comparators of kNumberCompare.
@@ -181,6 +189,10 @@ class Parser {
       switch (cur.peek()) {
       case ':': {
         cur.expect(':');
+        if (wildcard > 0 && (cur.peek() == ']' || cur.peek() == '-')) {
+          open_slice(i);  // "[a:]", "[a:-b]"
+          return;
+        }
         const uint64_t end = read_integer([](char e) { return e == ']'; });
         cur.expect(']');
         range(i, end, false);
@@ -211,6 +223,10 @@ class Parser {
       }
     } else if (c == ':') {
       cur.expect(':');
+      if (wildcard > 0 && cur.peek() == '-') {
+        open_slice(0);  // "[:-b]"
+        return;
+      }
       if (!std::isdigit(static_cast<unsigned char>(cur.peek())))
         throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Unexpected character in index, expected an integer");
       const uint64_t end = read_integer([](char e) { return e == ']'; });
@@ -228,6 +244,16 @@ class Parser {
           ++max_level;
         } else {
           cur.expect(':');
+          if (cur.peek() == '-') {
+            // "[-a:-b]": the reverse indexes a .. b+1
+            cur.expect('-');
+            const uint64_t b = read_integer([](char e) { return e == ']'; });
+            if (b == 0) throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Invalid reverse index 0");
+            if (b >= i) throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Empty index range");
+            cur.expect(']');
+            range(b, i, true);
+            return;
+          }
           cur.expect(']');
           range(0, i, true);
           return;
@@ -240,10 +266,7 @@ class Parser {
     } else if (c == '*') {
       if (wildcard == 0) throw cur.fail(GPJ_ERR_UNSUPPORTED_QUERY, "Unsupported wildcard expression");
       cur.expect('*');
-      cur.expect(']');
-      ir.op(kExpectAtMost);  // no silent truncation of longer arrays
-      ir.varint(wildcard);
-      range(0, wildcard, false);
+      open_slice(0, false);  // "[0:]": no silent truncation of longer arrays
       return;
     } else if (c == '?') {
       filter();
@@ -255,28 +278,48 @@ class Parser {
     if (cur.has_next()) next_expression();
   }
 
+  // "[a:]" and "[a:-b]" with the wildcard limit K: elements a .. a+K-1, each
+  // checked to exist and, for "[a:-b]", to be followed by at least b
+  // elements; an array with more than a+K+b elements raises the overflow
+  // status.  The cursor is after ':' ("[*]": after '*').
+  void open_slice(uint64_t start, bool from_end = true) {
+    uint64_t tail = 0;
+    if (from_end && cur.skip('-')) {
+      tail = read_integer([](char e) { return e == ']'; });
+      if (tail == 0) throw cur.fail(GPJ_ERR_MALFORMED_QUERY, "Invalid reverse index 0");
+    }
+    cur.expect(']');
+    ir.op(kExpectAtMost);
+    ir.varint(start + wildcard + tail);
+    range(start, start + wildcard, false, int64_t(tail));
+  }
+
   void multiple(const std::vector<uint64_t> &list) {
     uint64_t mm = max_level;
     for (size_t b = 0; b < list.size(); ++b) mm = branch(list[b], b + 1 == list.size(), mm, false);
     max_level = mm + 1;
   }
 
-  void range(uint64_t start, uint64_t end, bool reverse) {
+  void range(uint64_t start, uint64_t end, bool reverse, int64_t follow = -1) {
     uint64_t mm = max_level;
     if (reverse) {
       for (uint64_t i = end; i > start; --i) mm = branch(i, i == start + 1, mm, true);
     } else {
-      for (uint64_t i = start; i < end; ++i) mm = branch(i, i + 1 == end, mm, false);
+      for (uint64_t i = start; i < end; ++i) mm = branch(i, i + 1 == end, mm, false, follow);
     }
     max_level = mm + 1;
   }
 
   // query_compiler.cpp:335-364: one IR branch per index; every branch but the
   // last stores its result and climbs back to where it started.
-  uint64_t branch(uint64_t index, bool last, uint64_t mm, bool reverse) {
+  uint64_t branch(uint64_t index, bool last, uint64_t mm, bool reverse, int64_t follow = -1) {
     const uint64_t start_level = ir.level;
     if (reverse) ir.reverse_index(index);
     else ir.index(index);
+    if (follow >= 0) {
+      ir.op(kExpectFollowing);
+      ir.varint(uint64_t(follow));
+    }
     ir.down();
     cur.marks.push_back(cur.pos);
     const uint64_t saved = max_level;

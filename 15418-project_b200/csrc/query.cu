@@ -26,6 +26,7 @@ enum : uint8_t {
   OP_NUMBER_COMPARE = 0x0A,  // numeric filter: cmp byte, varint length, number text
   OP_DESCEND_KEY = 0x0B,     // "..name" as the last step: varint length, key bytes
   OP_EXPECT_AT_MOST = 0x0C,  // "[*]" element-count check: varint limit
+  OP_EXPECT_FOLLOWING = 0x0D,  // "[a:-b]": varint count of elements that must follow
 };
 
 // Last bitmap word read, per thread: consecutive searches of a record mostly
@@ -631,6 +632,30 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
       if (commas >= limit) raise_status(c, kQueryStatusOverflow);
       break;
     }
+    case OP_EXPECT_FOLLOWING: {
+      if constexpr (!kExt) return;
+      const int need = read_varint(c, qp);
+      if (need < 0 || !LEVEL_OK(level)) return;
+      // The element must exist (an empty array has no element 0) and be
+      // followed by `need` commas at this level before the closing bracket;
+      // otherwise it is among the last `need` (and so is every later one):
+      // the record is done.
+      const Pos lend = L.level_end(level);
+      const uint64_t *lvl = level_words(c, level);
+      Pos p = line_index;
+      while (p < lend && at(c, p) == ' ') ++p;
+      if (at(c, p) == ']') return;
+      p = line_index - 1;
+      int commas = 0;
+      steps = 0;
+      while (commas < need) {
+        if (++steps > max_steps) return;
+        p = next_struct(c, lbc, lend, Pos(p + 1), lvl);
+        if (at(c, p) != ',') return;
+        ++commas;
+      }
+      break;
+    }
     default:
       break;
     }
@@ -639,8 +664,9 @@ __device__ void run_record(const Rec<Pos> &c, const LevelState<Pos> &L, Pos line
 #undef LEVEL_OK
 }
 
-// kExt: the IR holds extension opcodes (numeric filters, "..name", "[*]"
-// checks); reference-syntax IR runs the variant without them.
+// kExt: the IR holds extension opcodes (numeric filters, "..name", the
+// element checks of "[*]" and the open slices); reference-syntax IR runs the
+// variant without them.
 template <typename Pos, typename OutT, bool kExt>
 __global__ void __launch_bounds__(256)
     query_kernel(const QueryLaunch q, const __grid_constant__ IrBlob ir, OutT *out, int nlev) {
@@ -735,7 +761,8 @@ int query_ir_levels(const uint8_t *ir, int len) {
       break;
     case OP_MOVE_TO_INDEX:
     case OP_MOVE_TO_INDEX_REVERSE:
-    case OP_EXPECT_AT_MOST: skip_varint(p, nullptr); break;
+    case OP_EXPECT_AT_MOST:
+    case OP_EXPECT_FOLLOWING: skip_varint(p, nullptr); break;
     case OP_NUMBER_COMPARE:
       ++p;  // comparator
       skip_varint(p, &n);
@@ -774,7 +801,8 @@ bool query_ir_uses_extensions(const uint8_t *ir, int len) {
     case OP_END: return false;
     case OP_NUMBER_COMPARE:
     case OP_DESCEND_KEY:
-    case OP_EXPECT_AT_MOST: return true;
+    case OP_EXPECT_AT_MOST:
+    case OP_EXPECT_FOLLOWING: return true;
     case OP_MOVE_TO_KEY:
     case OP_EXPRESSION_STRING_EQUALS: {
       const int n = skip_varint(p);

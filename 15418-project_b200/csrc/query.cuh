@@ -12,7 +12,8 @@ constexpr int kMaxQueryLevels = 16;   // orig.hpp:10 kMaxQueryLevels
 constexpr int kMaxQueryIrBytes = 4096;  // orig.hpp:11 kMaxQueryIrBytes
 
 // Status bit a query raises when a record had more results than its slots:
-// a "[*]" array longer than the wildcard limit, or more "..name" matches.
+// a "[*]" array or open slice longer than the wildcard limit, or more
+// "..name" matches.
 // Only IR with extension opcodes can raise it.  Kept clear of the indexer's
 // error bits (1, 2, 4), with which it shares the batch's error word.
 constexpr unsigned int kQueryStatusOverflow = 0x100u;
@@ -45,8 +46,9 @@ struct IrBlob {
 cudaError_t query_launch(const QueryLaunch &q, const IrBlob &ir, int grid,
                          int block, cudaStream_t stream);
 
-// True when the IR holds extension opcodes (numeric filters, "..name",
-// "[*]" element checks): those launch the interpreter variant that has them.
+// True when the IR holds extension opcodes (numeric filters, "..name", the
+// element checks of "[*]" and the open slices): those launch the
+// interpreter variant that has them.
 bool query_ir_uses_extensions(const uint8_t *ir, int len);
 
 // Batched query over every record of every file of a multi-file index build:

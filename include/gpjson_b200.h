@@ -100,7 +100,14 @@ int gpj_ctx_destroy(gpj_ctx *ctx);
  *  - numeric filters "[?(@<path> <op> <number>)]", op one of == != < <= > >=,
  *    an exact decimal comparison with a JSON number (a value that is not a
  *    number fails the filter; query_compiler.cpp:366-391 takes only
- *    == "string"). */
+ *    == "string");
+ *  - "[-a:-b]" (a > b >= 1): the reverse indexes a .. b+1, in the
+ *    reference's own IR (its parser accepts only "[-a:]",
+ *    query_compiler.cpp:256-286);
+ *  - K > 0: the open slices "[a:]", "[a:-b]" and "[:-b]": elements a ..
+ *    a+K-1 that are not among the last b, in K result slots; an array whose
+ *    slice holds more than K elements raises GPJ_QUERY_OVERFLOW.
+ * "[--" stays rejected with the reference's message. */
 int gpj_compile(const char *query, uint64_t wildcard_limit, uint8_t *h_ir,
                 uint64_t ir_capacity, uint64_t *ir_len, uint64_t *max_depth,
                 uint64_t *num_result_slots);

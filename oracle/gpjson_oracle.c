@@ -174,11 +174,13 @@ enum {
   OP_RESET_POSITION = 0x08,
   OP_EXPRESSION_STRING_EQUALS = 0x09,
   /* Extensions of this build (never emitted for the reference's syntax):
-   * numeric filters, recursive descent to a member name, and the element
-   * count check of a bounded "[*]". */
+   * numeric filters, recursive descent to a member name, the element count
+   * check of a bounded "[*]" or open slice, and the check that an element is
+   * not among the last b of its array ("[a:-b]"). */
   OP_NUMBER_COMPARE = 0x0A,
   OP_DESCEND_KEY = 0x0B,
-  OP_EXPECT_AT_MOST = 0x0C
+  OP_EXPECT_AT_MOST = 0x0C,
+  OP_EXPECT_FOLLOWING = 0x0D
 };
 #define ORC_MAX_LEVELS 16 /* query.cu:20 MAX_NUM_LEVELS */
 
@@ -739,6 +741,28 @@ static void query_record(qctx *c, int64_t line_start, int64_t line_end,
         ++commas;
       }
       if (limit > 0 && commas >= limit) c->status |= ORC_STATUS_OVERFLOW;
+      break;
+    }
+
+    case OP_EXPECT_FOLLOWING: { /* extension: "[a:-b]", after MOVE_TO_INDEX */
+      const int need = read_varint(c, &query_pos);
+      if (need < 0 || !LEVEL_OK(current_level)) return;
+      /* The element must exist (an empty array has no element 0) and be
+       * followed by `need` commas at this level before the closing bracket;
+       * otherwise it is among the last `need` (and so is every later one):
+       * the record is done. */
+      int64_t p = line_index;
+      while (p < level_end[current_level] && at(c, p) == ' ') ++p;
+      if (at(c, p) == ']') return;
+      p = line_index - 1;
+      int commas = 0;
+      steps = 0;
+      while (commas < need) {
+        if (++steps > max_steps) return;
+        p = find_next_structural_char(c, level_end[current_level], p + 1, current_level);
+        if (at(c, p) != ',') return;
+        ++commas;
+      }
       break;
     }
 

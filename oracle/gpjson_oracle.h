@@ -64,10 +64,12 @@ int orc_query(const uint8_t *in, uint64_t n, const int64_t *NL,
 
 /* orc_query that also returns status bits: ORC_STATUS_OVERFLOW when a record
  * had more results than num_results (only the extension opcodes can: a
- * recursive descent with more matches, or a "[*]" array longer than its
- * limit).  Extensions of this build, rejected by the reference's compiler:
- * 0x0A NUMBER_COMPARE (numeric filter), 0x0B DESCEND_KEY ("..name" as the
- * last step), 0x0C EXPECT_AT_MOST ("[*]" element-count check). */
+ * recursive descent with more matches, or a "[*]" array or open slice longer
+ * than its limit).  Extensions of this build, rejected by the reference's
+ * compiler: 0x0A NUMBER_COMPARE (numeric filter), 0x0B DESCEND_KEY ("..name"
+ * as the last step), 0x0C EXPECT_AT_MOST (element-count check of "[*]" and
+ * the open slices), 0x0D EXPECT_FOLLOWING (an element of "[a:-b]" must be
+ * followed by b more). */
 #define ORC_STATUS_OVERFLOW 1u
 /* A device assert of the reference's query kernel would fire on this input
  * (src/gpjson/query/kernels/orig/query.cu:230, 265, 276, 290, 321, 334, 370,

@@ -14,7 +14,7 @@ OPS = {0: "END", 1: "STORE_RESULT", 2: "MOVE_UP", 3: "MOVE_DOWN", 4: "MOVE_TO_KE
        5: "MOVE_TO_INDEX", 6: "MOVE_TO_INDEX_REVERSE", 7: "MARK_POSITION",
        8: "RESET_POSITION", 9: "EXPRESSION_STRING_EQUALS",
        # extensions of this build (the reference rejects these queries)
-       10: "NUMBER_COMPARE", 11: "DESCEND_KEY", 12: "EXPECT_AT_MOST"}
+       10: "NUMBER_COMPARE", 11: "DESCEND_KEY", 12: "EXPECT_AT_MOST", 13: "EXPECT_FOLLOWING"}
 CMPS = {0: "==", 1: "!=", 2: "<", 3: "<=", 4: ">", 5: ">="}
 
 
@@ -44,7 +44,8 @@ def decode(ir: bytes):
             n = varint()
             ins["string"] = ir[i:i + n].decode()
             i += n
-        elif op in ("MOVE_TO_INDEX", "MOVE_TO_INDEX_REVERSE", "EXPECT_AT_MOST"):
+        elif op in ("MOVE_TO_INDEX", "MOVE_TO_INDEX_REVERSE", "EXPECT_AT_MOST",
+                    "EXPECT_FOLLOWING"):
             ins["integer"] = varint()
         out.append(ins)
         if op == "END":
@@ -133,17 +134,53 @@ def test_wildcard_extension_is_off_by_default(gpj):
         gpj.compile("$.entities.hashtags[*].text")
     w = gpj.compile("$.entities.hashtags[*].text", wildcard_limit=8)
     r = gpj.compile("$.entities.hashtags[0:8].text")
-    # "[*]" = an element-count check, then exactly the IR of "[0:8]"
+    # "[*]" = an element-count check, then the IR of "[0:8]" with an
+    # element-exists check after each index step
     wi, ri = decode(w.ir_bytes), decode(r.ir_bytes)
     assert wi[4] == {"opcode": "EXPECT_AT_MOST", "integer": 8}
-    assert wi[:4] + wi[5:] == ri
+    checks = [i for i, x in enumerate(wi) if x["opcode"] == "EXPECT_FOLLOWING"]
+    assert len(checks) == 8 and all(wi[i - 1]["opcode"] == "MOVE_TO_INDEX" and
+                                     wi[i]["integer"] == 0 for i in checks)
+    assert [x for i, x in enumerate(wi) if i != 4 and i not in checks] == ri
     assert (w.max_depth, w.num_result_slots) == (r.max_depth, r.num_result_slots)
+
+
+def test_slices_from_the_end_compile(gpj):
+    # "[-a:-b]": the reference's reverse-index IR, no extension opcode
+    c = gpj.compile("$.a[-4:-1]")
+    ins = decode(c.ir_bytes)
+    assert [x["integer"] for x in ins if x["opcode"] == "MOVE_TO_INDEX_REVERSE"] == [4, 3, 2]
+    assert (c.max_depth, c.num_result_slots) == (2, 3)
+    assert not any(x["opcode"] in ("EXPECT_AT_MOST", "EXPECT_FOLLOWING") for x in ins)
+    # open slices need the wildcard limit K: K branches, count check a+K+b
+    c = gpj.compile("$.a[2:-3].b", wildcard_limit=4)
+    ins = decode(c.ir_bytes)
+    assert ins[2] == {"opcode": "EXPECT_AT_MOST", "integer": 9}
+    assert [x["integer"] for x in ins if x["opcode"] == "MOVE_TO_INDEX"] == [2, 3, 4, 5]
+    assert [x["integer"] for x in ins if x["opcode"] == "EXPECT_FOLLOWING"] == [3] * 4
+    assert (c.max_depth, c.num_result_slots) == (3, 4)
+    assert gpj.compile("$.a[:-1]", wildcard_limit=2).num_result_slots == 2
+    assert gpj.compile("$.a[5:]", wildcard_limit=3).num_result_slots == 3
+    # without K the reference's errors stand
+    with pytest.raises(ValueError):
+        gpj.compile("$.a[5:]")
+    with pytest.raises(gpj.MalformedQueryError, match="expected an integer"):
+        gpj.compile("$.a[:-1]")
+    with pytest.raises(gpj.MalformedQueryError, match="Empty index range"):
+        gpj.compile("$.a[-1:-2]")
+    with pytest.raises(gpj.MalformedQueryError, match="Invalid reverse index 0"):
+        gpj.compile("$.a[1:-0]", wildcard_limit=2)
+    with pytest.raises(gpj.MalformedQueryError):
+        gpj.compile("$.a[*-1]", wildcard_limit=2)
+    with pytest.raises(gpj.UnsupportedQueryError, match="Unsupported last n elements"):
+        gpj.compile("$.a[--1]", wildcard_limit=2)
 
 
 def test_reference_syntax_never_uses_extension_opcodes(gpj):
     for case in KATS["compiler"]["cases"]:
         if "query" in case:
-            assert all(ins["opcode"] not in ("NUMBER_COMPARE", "DESCEND_KEY", "EXPECT_AT_MOST")
+            assert all(ins["opcode"] not in ("NUMBER_COMPARE", "DESCEND_KEY", "EXPECT_AT_MOST",
+                                             "EXPECT_FOLLOWING")
                        for ins in decode(gpj.compile(case["query"]).ir_bytes))
 
 

@@ -1,6 +1,7 @@
 """Query-language extensions on the GPU vs the CPU oracle (bit-exact):
-numeric filters, "..name", and the "[*]" element-count check with its
-overflow status (context status word, gpj_query_host error, batch error
+numeric filters, "..name", slices counted from the end and open slices, and
+the element-count check of "[*]" and the open slices with its overflow
+status (context status word, gpj_query_host error, batch error
 word).  The oracle's semantics for these are pinned on CPU against an
 independent JSON evaluation (tests/test_query_ext_host.py)."""
 import numpy as np
@@ -18,6 +19,8 @@ EXT_QUERIES = [
     ("$.id[?(@ >= 5E17)]", 0), ("$.user[?(@.followers_count >= 10000)].screen_name", 0),
     ("$.user.statuses_count[?(@ != 35105)]", 0), ("$.place.bounding_box.coordinates[0][0][0][0][?(@ < 0)]", 0),
     ("$.entities.hashtags[*].text", 8), ("$.entities.hashtags[*].indices[1]", 8),
+    ("$.entities.hashtags[-3:-1].text", 0), ("$.entities.hashtags[1:].text", 4),
+    ("$.entities.hashtags[:-1].indices[0]", 6), ("$.entities.hashtags[1:-1]", 3),
 ]
 
 
@@ -119,3 +122,18 @@ def test_batch_extension_queries_and_overflow(gpj):
             got = R[out_off:out_off + lines * c.num_result_slots * 2].astype(np.int64)
             want = oracle.OracleIndex(d, lv).query(c.ir_bytes, c.num_result_slots, base)
             np.testing.assert_array_equal(got.reshape(lines, -1, 2), want, err_msg=str(f))
+
+
+def test_slices_on_arrays_match_oracle(cuda_ctx, gpj):
+    """Every slice form over arrays of 0-11 elements, empty arrays included."""
+    from test_query_ext_host import SLICE_CASES, array_records
+    data = np.frombuffer(array_records(11, 4000), np.uint8).copy()
+    comp = [gpj.compile(q, wildcard_limit=k) for q, _, _, _, _, k in SLICE_CASES]
+    L = max(c.max_depth for c in comp)
+    want_ix = oracle.OracleIndex(data, L)
+    for c, (got, status) in zip(comp, _gpu_query(cuda_ctx, gpj, data, comp, L)):
+        want = want_ix.query(c.ir_bytes, c.num_result_slots)
+        np.testing.assert_array_equal(got, want, err_msg=c.query_text)
+        overflow = want_ix.last_status & oracle.OracleIndex.STATUS_OVERFLOW
+        assert status == (gpj.GPJ_QUERY_OVERFLOW if overflow else 0), c.query_text
+        assert (got[:, :, 0] >= 0).sum() > 100, c.query_text

@@ -190,3 +190,87 @@ def test_wildcard_limit_overflow_status(gpj, tweets):
             want.append([x["text"] for x in h[:k]] if h else [])
         got = _values(tweets, res)
         assert got == want
+
+
+# ---- slices counted from the end, and open slices ----
+
+def array_records(seed: int = 7, count: int = 600) -> bytes:
+    """Records with arrays of 0-11 elements (objects and numbers), nested
+    pairs, and both compact and spaced separators."""
+    rng = np.random.default_rng(seed)
+    lines = []
+    for i in range(count):
+        arr = []
+        for _ in range(int(rng.integers(0, 12))):
+            if rng.random() < 0.7:
+                arr.append({"v": int(rng.integers(-99, 99)), "s": "x" * int(rng.integers(0, 5))})
+            else:
+                arr.append(int(rng.integers(0, 1000)))
+        rec = {"id": i, "a": arr, "b": {"c": [[j, j + 1] for j in range(int(rng.integers(0, 5)))]}}
+        seps = (",", ":") if i % 2 else (", ", ": ")
+        lines.append(json.dumps(rec, separators=seps))
+    return "\n".join(lines).encode()
+
+
+@pytest.fixture(scope="module")
+def arrays():
+    return array_records()
+
+
+def _apply(values, rest):
+    """The remaining steps over each selected element; a failed step ends the
+    record (the reference abandons its remaining slots)."""
+    out = []
+    for x in values:
+        if rest is None:
+            out.append(x)
+            continue
+        kind, arg = rest
+        if kind == "key" and isinstance(x, dict) and arg in x:
+            out.append(x[arg])
+        elif kind == "index" and isinstance(x, list) and arg < len(x):
+            out.append(x[arg])
+        else:
+            break
+    return out
+
+
+SLICE_CASES = [
+    ("$.a[-3:-1]", ["a"], -3, -1, None, 0),
+    ("$.a[-5:-2].v", ["a"], -5, -2, ("key", "v"), 0),
+    ("$.a[1:]", ["a"], 1, None, None, 4),
+    ("$.a[0:]", ["a"], 0, None, None, 3),
+    ("$.a[2:-1]", ["a"], 2, -1, None, 3),
+    ("$.a[1:-3].v", ["a"], 1, -3, ("key", "v"), 5),
+    ("$.a[:-2]", ["a"], 0, -2, None, 6),
+    ("$.b.c[:-1][1]", ["b", "c"], 0, -1, ("index", 1), 3),
+    ("$.b.c[1:][0]", ["b", "c"], 1, None, ("index", 0), 2),
+    ("$.a[*]", ["a"], 0, None, None, 5),
+]
+
+
+@pytest.mark.parametrize("query,path,a,b,rest,k", SLICE_CASES)
+def test_slices_from_the_end(gpj, arrays, query, path, a, b, rest, k):
+    c = gpj.compile(query, wildcard_limit=k)
+    ix = oracle.OracleIndex(arrays, c.max_depth)
+    res = ix.query(c.ir_bytes, c.num_result_slots)
+    got = _values(arrays, res)
+    want, overflow = [], False
+    for rec in _records(arrays):
+        arr = _get(_loads(rec), path) if rec else None
+        if not isinstance(arr, list):
+            want.append([])
+            continue
+        n = len(arr)
+        if a < 0:
+            # reverse indexes -a .. -b-1: every one must exist
+            sel = arr[n + a:n + b] if n >= -a else []
+        else:
+            end = n + b if b is not None else n
+            sel = arr[a:end] if a < n else []
+            overflow |= len(sel) > k
+            sel = sel[:k]
+        want.append(_apply(sel, rest))
+    assert got == want
+    assert sum(map(len, want)) > 100
+    assert bool(ix.last_status & oracle.OracleIndex.STATUS_OVERFLOW) == overflow
