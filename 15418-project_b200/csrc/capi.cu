@@ -14,6 +14,9 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <unordered_map>
+#include <utility>
+#include <vector>
 
 struct gpj_ctx {
   int device = 0;
@@ -40,6 +43,11 @@ struct gpj_ctx {
   void *stage = nullptr;
   cudaEvent_t stage_done[3] = {nullptr, nullptr, nullptr};
   int stage_next = 0;
+  // gpj_index_build allocations: sizes of the live ones, and the ones
+  // gpj_index_free released, kept for the next build of a similar size (a
+  // cudaMalloc/cudaFree pair of tens of MB costs milliseconds)
+  std::unordered_map<void *, uint64_t> index_live;
+  std::vector<std::pair<void *, uint64_t>> index_spare;
 };
 
 namespace {
@@ -313,20 +321,73 @@ int read_summary(gpj_ctx *ctx, uint64_t n, cudaStream_t stream, uint64_t *lines,
   return GPJ_OK;
 }
 
-void release_index(gpj_index *ix) {
-  if (ix->owner != nullptr) cudaFree(ix->owner);
+constexpr size_t kSpareIndexBlocks = 4;
+
+// Releases an index allocation.  With its context the block is kept for
+// reuse after a device synchronisation (what cudaFree implies: work still
+// reading the index has finished); the largest spare goes once more than
+// kSpareIndexBlocks are kept.
+void release_index(gpj_ctx *ctx, gpj_index *ix) {
+  void *mem = ix->owner;
   std::memset(ix, 0, sizeof(*ix));
+  if (mem == nullptr) return;
+  auto it = ctx != nullptr ? ctx->index_live.find(mem) : decltype(ctx->index_live)::iterator{};
+  if (ctx == nullptr || it == ctx->index_live.end() || cudaSetDevice(ctx->device) != cudaSuccess ||
+      cudaDeviceSynchronize() != cudaSuccess) {
+    if (ctx != nullptr && it != ctx->index_live.end()) ctx->index_live.erase(it);
+    cudaFree(mem);
+    return;
+  }
+  ctx->index_spare.emplace_back(mem, it->second);
+  ctx->index_live.erase(it);
+  if (ctx->index_spare.size() > kSpareIndexBlocks) {
+    auto big = std::max_element(ctx->index_spare.begin(), ctx->index_spare.end(),
+                                [](const auto &a, const auto &b) { return a.second < b.second; });
+    cudaFree(big->first);
+    ctx->index_spare.erase(big);
+  }
+}
+
+// One device block of at least `bytes`: the smallest spare that is not more
+// than 1.5x (+ 16 MiB) larger, else a new cudaMalloc.
+int take_index_block(gpj_ctx *ctx, uint64_t bytes, void **mem) {
+  *mem = nullptr;
+  auto best = ctx->index_spare.end();
+  for (auto it = ctx->index_spare.begin(); it != ctx->index_spare.end(); ++it) {
+    if (it->second >= bytes && it->second <= bytes + bytes / 2 + (16u << 20) &&
+        (best == ctx->index_spare.end() || it->second < best->second))
+      best = it;
+  }
+  uint64_t got = bytes;
+  if (best != ctx->index_spare.end()) {
+    *mem = best->first;
+    got = best->second;
+    ctx->index_spare.erase(best);
+  } else {
+    cudaError_t e = cudaMalloc(mem, bytes);
+    if (e == cudaErrorMemoryAllocation && !ctx->index_spare.empty()) {
+      // the spares may be what stands in the way
+      (void)cudaGetLastError();
+      for (auto &b : ctx->index_spare) cudaFree(b.first);
+      ctx->index_spare.clear();
+      e = cudaMalloc(mem, bytes);
+    }
+    GPJ_CUDA(e, "cudaMalloc index");
+  }
+  ctx->index_live[*mem] = got;
+  return GPJ_OK;
 }
 
 // Carves one allocation into the index arrays.
-int alloc_index(gpj_index *ix, uint64_t n, int levels, bool eq, uint64_t nl_cap) {
+int alloc_index(gpj_ctx *ctx, gpj_index *ix, uint64_t n, int levels, bool eq, uint64_t nl_cap) {
   const uint64_t W = (n + 63u) / 64u;
   const uint64_t s_bytes = round256(W * 8u);
   const uint64_t lb_bytes = round256(W * 8u * uint64_t(levels));
   const uint64_t nl_bytes = round256(nl_cap * 8u);
   const uint64_t eq_bytes = eq ? 2u * s_bytes : 0u;
   void *mem = nullptr;
-  GPJ_CUDA(cudaMalloc(&mem, s_bytes + lb_bytes + nl_bytes + eq_bytes + 256u), "cudaMalloc index");
+  const int rc = take_index_block(ctx, s_bytes + lb_bytes + nl_bytes + eq_bytes + 256u, &mem);
+  if (rc != GPJ_OK) return rc;
   auto *p = static_cast<unsigned char *>(mem);
   ix->owner = mem;
   ix->d_string = reinterpret_cast<uint64_t *>(p);
@@ -471,6 +532,7 @@ int gpj_ctx_destroy(gpj_ctx *ctx) {
   cudaFree(ctx->compact_scratch);
   cudaFree(ctx->d_status);
   cudaFreeHost(ctx->pinned);
+  for (auto &b : ctx->index_spare) cudaFree(b.first);
   if (ctx->piece_ready) cudaEventDestroy(ctx->piece_ready);
   for (auto &e : ctx->stage_done)
     if (e) cudaEventDestroy(e);
@@ -513,7 +575,7 @@ int gpj_index_build(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_bytes,
   const bool eq = (flags & GPJ_INDEX_EMIT_ESCAPE_QUOTE) != 0;
   uint64_t cap = nl_capacity_guess(size_bytes);
   for (int attempt = 0; attempt < 2; ++attempt) {
-    rc = alloc_index(out, size_bytes, num_levels, eq, cap);
+    rc = alloc_index(ctx, out, size_bytes, num_levels, eq, cap);
     if (rc != GPJ_OK) return rc;
     out->d_input = d_input;
     out->size_bytes = size_bytes;
@@ -522,14 +584,14 @@ int gpj_index_build(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_bytes,
     int in_string = 0, depth = -1;
     if (rc == GPJ_OK) rc = read_summary(ctx, size_bytes, stream, &lines, &in_string, &depth);
     if (rc != GPJ_OK) {
-      release_index(out);
+      release_index(ctx, out);
       return rc;
     }
     out->num_lines = lines;
     out->final_in_string = in_string;
     out->final_depth = depth;
     if (lines <= cap) return GPJ_OK;
-    release_index(out);
+    release_index(ctx, out);
     cap = lines;  // exact size, second pass
   }
   return fail(GPJ_ERR_IMPLEMENTATION, "newline capacity retry failed");
@@ -569,8 +631,7 @@ int gpj_index_build_async(gpj_ctx *ctx, const uint8_t *d_input, uint64_t size_by
 }
 
 int gpj_index_free(gpj_ctx *ctx, gpj_index *index) {
-  (void)ctx;
-  if (index != nullptr) release_index(index);
+  if (index != nullptr) release_index(ctx, index);
   return GPJ_OK;
 }
 

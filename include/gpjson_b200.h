@@ -173,7 +173,11 @@ int gpj_index_build_noalloc(const uint8_t *d_input, uint64_t size_bytes,
 int gpj_copy_to_device(gpj_ctx *ctx, void *d_dst, const void *h_src, uint64_t size_bytes,
                        void *stream);
 
-/* Releases what gpj_index_build allocated. */
+/* Releases what gpj_index_build allocated.  Like cudaFree it waits for the
+ * device to finish the work already queued.  The context keeps up to four
+ * released blocks for later builds of a similar size (no cudaMalloc then);
+ * gpj_ctx_destroy frees them.  Free an index with the context that built it,
+ * before that context is destroyed, or with ctx = NULL (plain cudaFree). */
 int gpj_index_free(gpj_ctx *ctx, gpj_index *index);
 
 /* Runs one compiled query over every record of an indexed partition and

@@ -223,3 +223,45 @@ def test_lookback_wait_runs_out_and_reports_timeout(cuda_ctx, gpj):
         cuda_ctx.build_index(ptr, 1000, 2, diag)
     # the same context, a normal build: bit-exact again
     assert_same(gpu_index(cuda_ctx, gpj, data, 2), oracle.OracleIndex(data, 2))
+
+
+def test_released_blocks_are_reused(gpj):
+    """gpj_index_free keeps released blocks in the context: a later build of
+    a similar size takes one (no cudaMalloc) and its indexes are bit-exact;
+    a block more than 1.5x (+ 16 MiB) too large is left alone.  An index
+    freed after its context is gone is released with a null context."""
+    from gpjson_b200 import datagen
+    big = datagen.tweets(17, 48 << 20)
+    small = datagen.tweets(18, 2 << 20)
+    tb, pb = to_device(big)
+    ts, ps = to_device(small)
+    want_small = oracle.OracleIndex(small, 3)
+    with gpj.Context(0) as ctx:
+        a = ctx.build_index(pb, big.size, 3)
+        block_a, first = a.owner, index_arrays(a)
+        ctx.free_index(a)
+        a = ctx.build_index(pb, big.size, 3)
+        assert a.owner == block_a
+        again = index_arrays(a)
+        for k in ("S", "LB", "NL"):
+            np.testing.assert_array_equal(again[k], first[k], err_msg=k)
+        s = ctx.build_index(ps, small.size, 3)  # the big block is live
+        block_s = s.owner
+        assert block_s != block_a
+        ctx.free_index(s)
+        ctx.free_index(a)
+        s = ctx.build_index(ps, small.size, 3)  # the small block fits best
+        assert s.owner == block_s
+        got = index_arrays(s)
+        np.testing.assert_array_equal(got["S"], want_small.S)
+        np.testing.assert_array_equal(got["LB"], want_small.LB)
+        np.testing.assert_array_equal(got["NL"][:s.num_lines], want_small.NL)
+        ctx.free_index(s)
+        tiny = datagen.tweets(19, 64 << 10)
+        tt, pt = to_device(tiny)
+        t = ctx.build_index(pt, tiny.size, 3)  # the big block is too large
+        assert t.owner not in (block_a,)
+        ctx.free_index(t)
+        late = ctx.build_index(pb, big.size, 3)
+    ctx.free_index(late)  # context closed: plain cudaFree
+    assert late.owner is None
