@@ -356,12 +356,13 @@ struct PipeSmem {
 
 // Shared-memory staging of the leveled bitmaps (phase B): per warp and
 // level, one 64-bit slot for each of the warp's 64 words; a lane only ever
-// touches the slots of its own two words.
+// touches the slots of its own two words.  Level LMAX is a sink for the
+// masks of depths that are not stored, so the walk writes without a branch.
 constexpr int kSharedLevels = 8;  // LMAX up to this stages in shared memory
 template <int NT, int LMAX>
 struct LevelScratch {
   static constexpr int NW = NT / 32;
-  uint64_t lb[NW][LMAX][64];
+  uint64_t lb[NW][LMAX + 1][64];
 };
 
 // One thread's row between phase A and phase B.
@@ -709,7 +710,10 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
     slot64[l * 64 + 1] = 0ull;
   }
   uint32_t *slot = reinterpret_cast<uint32_t *>(slot64);  // [level * 128 + quarter]
-  int d = depth0;
+  // The signed-char depth is kept modulo 256 in the low byte of d: depths 0
+  // .. LMAX-1 are the bytes 0 .. LMAX-1, negative depths the bytes 128 ..
+  // 255, and every byte from LMAX up selects the sink level.
+  uint32_t d = uint32_t(depth0);
 #pragma unroll
   for (int h = 0; h < 4; ++h) {
     const uint64_t Ow = h < 2 ? O0 : O1, Cw = h < 2 ? C0 : C1, Pw = h < 2 ? P0 : P1;
@@ -720,18 +724,18 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
     while (ev) {  // branch-free body: lanes only differ in the trip count
       const uint32_t bit = ev & (0u - ev);
       const uint32_t below = bit - 1u;
-      acc |= Pm & below & ~done;
-      const bool open = (O & bit) != 0u;
-      const uint32_t m = acc | (bit & ~O);  // a closing bracket joins its level
-      if (m != 0u && unsigned(d) < unsigned(LMAX)) slot[d * 128 + h] |= m;
-      d = int(int8_t(uint8_t(open ? d + 1 : d - 1)));
-      acc = open ? bit : 0u;
+      const uint32_t ob = O & bit;  // the bit if the event opens a level
+      // separators since the last event, the opening bracket that started
+      // this run, and a closing bracket, which joins the level it closes
+      const uint32_t m = acc | (Pm & below & ~done) | (bit ^ ob);
+      slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= m;
+      d += ob ? 1u : 0xFFFFFFFFu;
+      acc = ob;
       done = below | bit;
-      ev &= ev - 1u;
+      ev ^= bit;
     }
     // separators after the quarter's last event
-    const uint32_t m = acc | (Pm & ~done);
-    if (m != 0u && unsigned(d) < unsigned(LMAX)) slot[d * 128 + h] |= m;
+    slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= acc | (Pm & ~done);
   }
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
