@@ -720,22 +720,24 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
     const uint32_t O = uint32_t((h & 1) ? (Ow >> 32) : Ow);
     const uint32_t C = uint32_t((h & 1) ? (Cw >> 32) : Cw);
     const uint32_t Pm = uint32_t((h & 1) ? (Pw >> 32) : Pw);
-    uint32_t ev = O | C, acc = 0u, done = 0u;
+    // Between two consecutive events the only bits of P | O are the
+    // separators and, when the earlier event opens a level, its own bit:
+    // exactly the bits of that run's level.
+    const uint32_t PO = Pm | O;
+    uint32_t ev = O | C, below_prev = 0u;
     while (ev) {  // branch-free body: lanes only differ in the trip count
       const uint32_t bit = ev & (0u - ev);
       const uint32_t below = bit - 1u;
-      const uint32_t ob = O & bit;  // the bit if the event opens a level
-      // separators since the last event, the opening bracket that started
-      // this run, and a closing bracket, which joins the level it closes
-      const uint32_t m = acc | (Pm & below & ~done) | (bit ^ ob);
+      // the run since the last event, and a closing bracket, which joins
+      // the level it closes
+      const uint32_t m = ((below ^ below_prev) & PO) | (bit & ~O);
       slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= m;
-      d += ob ? 1u : 0xFFFFFFFFu;
-      acc = ob;
-      done = below | bit;
+      d += (O & bit) ? 1u : 0xFFFFFFFFu;
+      below_prev = below;
       ev ^= bit;
     }
-    // separators after the quarter's last event
-    slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= acc | (Pm & ~done);
+    // the run after the quarter's last event
+    slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= PO & ~below_prev;
   }
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
