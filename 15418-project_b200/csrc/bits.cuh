@@ -56,8 +56,11 @@ __device__ __forceinline__ uint64_t escaped_bits(uint64_t bs, uint32_t carry_in)
   // Adding 1 at every odd start ripples through that run and clears it, so
   // what stays set under b are the runs that start on even bits.
   const uint64_t even_runs = (b + (starts & ~kEven)) & b;
-  const uint64_t odd_runs = b & ~even_runs;
-  return ((even_runs << 1) & ~kEven) | ((odd_runs << 1) & kEven) | cin;
+  // escaped: the odd positions after an even-started run, the even positions
+  // after an odd-started one -- the run bits on the other parity, shifted up
+  // once (one three-input mask per half instead of two shifts and masks)
+  const uint64_t pre = (even_runs & kEven) | (b & ~even_runs & ~kEven);
+  return (pre << 1) | cin;
 }
 
 // Carry the reference passes from a word to the next: parity of the run of

@@ -329,6 +329,8 @@ struct StageMeta {  // written by the control warp with each fill
   uint32_t tile;    // kEndTile: no more tiles for this CTA
   uint32_t file_idx;
   uint32_t halo;    // escape carry into the tile
+  uint32_t valid;   // bytes of the file in the tile
+  uint32_t smem_rows;  // rows 0 .. smem_rows-1 are read from the staged copy
   uint32_t pad;
   IndexFile F;
 };
@@ -339,7 +341,17 @@ struct TileMeta {  // a tile between its phase A and its phase B
   uint32_t par, dd, nl;  // tile aggregate: string parity, packed depth sums, newlines
   uint32_t c_in, d_in;   // prefix from the look-back
   unsigned long long n_in;
+  // Where phase B writes, computed once per tile: the file's S and level-0
+  // words from the tile's first word on, the file's word count and the
+  // tile's first word.  store_flags: kTileInside when every word of the
+  // tile lies inside the file (the stores need no bounds check), kTileSAligned
+  // when the S row of every thread starts on 16 bytes, and bit
+  // kTileLevelAligned + l when level l's rows do.
+  uint64_t *S_tile, *LB_tile;
+  uint64_t W, lw_tile;
+  uint32_t store_flags;
 };
+constexpr uint32_t kTileInside = 1u, kTileSAligned = 2u, kTileLevelAligned = 8u;
 
 template <int NT>
 struct PipeSmem {
@@ -474,10 +486,19 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
     halo = uint32_t(__clzll(static_cast<long long>(not_bs))) & 1u;
   }
   if (lane == 0) {
+    // the tile's bytes of the file, and the rows the compute threads read
+    // from the staged copy (whole rows inside the file and the tensor map)
+    const uint64_t byte0 = uint64_t(t - F.first_tile) * TILE_BYTES;
+    const uint32_t valid = uint32_t(min(TILE_BYTES, F.n - byte0));
+    uint32_t smem_rows = 0;
+    if (kTma && row0 < P.full_rows)
+      smem_rows = uint32_t(min(uint64_t(valid / 128u), P.full_rows - row0));
     sm.stage[s].tile = t;
     sm.stage[s].file_idx = f;
     sm.stage[s].F = F;
     sm.stage[s].halo = halo;
+    sm.stage[s].valid = valid;
+    sm.stage[s].smem_rows = smem_rows;
     mbar_arrive(full);
   }
   tile_out = t;
@@ -556,29 +577,20 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
   const IndexFile F = m.F;
   const uint32_t ktile = tile - F.first_tile;
   const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
-  const uint64_t valid = min(TILE_BYTES, F.n - byte0);
-  const uint8_t *fin = P.in + F.in_off;
-  const int64_t row0 = int64_t((F.in_off + byte0) / 128u);
-  const uint64_t row_byte = uint64_t(tid) * 128u;
+  const uint32_t valid = m.valid;
+  const uint32_t row_byte = uint32_t(tid) * 128u;
   const uint64_t lw0 = byte0 / 64u + 2u * uint64_t(tid);
-  const bool row_in_smem =
-      kTma && row_byte + 128u <= valid && row0 + tid < int64_t(P.full_rows);
+  const bool row_in_smem = kTma && uint32_t(tid) < m.smem_rows;
+  // rows past the end of the file read as zero bytes (no class)
+  const uint32_t lim = valid > row_byte ? valid - row_byte : 0u;
+  const uint8_t *rp = P.in + F.in_off + byte0 + row_byte;
   uint32_t r[16];
-  WordClasses c0, c1;
-  if (row_in_smem) {
-    load_word_smem(sm.tiles[s], tid, 0, r);
-    c0 = classify64(r);
-    load_word_smem(sm.tiles[s], tid, 1, r);
-    c1 = classify64(r);
-  } else {
-    // rows past the end of the file read as zero bytes (no class)
-    const uint64_t lim = valid > row_byte ? valid - row_byte : 0u;
-    const uint8_t *rp = fin + byte0 + row_byte;
-    load_word_global(rp, lim, 0, r);
-    c0 = classify64(r);
-    load_word_global(rp, lim, 64, r);
-    c1 = classify64(r);
-  }
+  if (row_in_smem) load_word_smem(sm.tiles[s], tid, 0, r);
+  else load_word_global(rp, lim, 0, r);
+  const WordClasses c0 = classify64(r);
+  if (row_in_smem) load_word_smem(sm.tiles[s], tid, 1, r);
+  else load_word_global(rp, lim, 64, r);
+  const WordClasses c1 = classify64(r);
   const uint32_t tp0 = trailing_escape_parity(c0.bs);
   const uint32_t tp1 = trailing_escape_parity(c1.bs);
   if (lane == 31) sm.last_tp[warp] = tp1;
@@ -671,6 +683,18 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
     tm.par = tile_par;
     tm.dd = tile_dd;
     tm.nl = tile_nl;
+    const uint64_t W = (F.n + 63u) / 64u;
+    const uint64_t lw_tile = byte0 / 64u;
+    tm.W = W;
+    tm.lw_tile = lw_tile;
+    tm.S_tile = P.S + F.s_off + lw_tile;
+    tm.LB_tile = P.LB + F.lb_off + lw_tile;
+    uint32_t flags = lw_tile + 2u * NT <= W ? kTileInside : 0u;
+    if ((reinterpret_cast<uintptr_t>(tm.S_tile) & 15u) == 0) flags |= kTileSAligned;
+    for (int l = 0; l < F.levels && l < 24; ++l)
+      if ((reinterpret_cast<uintptr_t>(tm.LB_tile + uint64_t(l) * W) & 15u) == 0)
+        flags |= 1u << (kTileLevelAligned + l);
+    tm.store_flags = flags;
     mbar_arrive(smem_u32(&sm.agg[k & 1u]));
   }
   st.op0 = c0.op;
@@ -750,7 +774,6 @@ template <int LMAX, int NT>
 __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
                                         LevelScratch<NT, LMAX> &ls, uint32_t k,
                                         const RowState &st) {
-  constexpr uint64_t TILE_BYTES = uint64_t(NT) * 128u;
   const int tid = threadIdx.x;
   const int j = int(k & 1u);
   if (!mbar_wait(smem_u32(&sm.pref[j]), (k >> 1) & 1u, &sm.abort)) {
@@ -759,11 +782,10 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
     return;
   }
   const TileMeta &tm = sm.tm[j];
-  const IndexFile F = tm.F;
-  const uint32_t ktile = tm.tile - F.first_tile;
-  const uint64_t byte0 = uint64_t(ktile) * TILE_BYTES;
-  const uint64_t W = (F.n + 63u) / 64u;
-  const uint64_t lw0 = byte0 / 64u + 2u * uint64_t(tid);
+  const uint64_t W = tm.W;
+  const uint64_t lw0 = tm.lw_tile + 2u * uint64_t(tid);
+  const int levels = tm.F.levels;
+  const uint32_t flags = tm.store_flags;
   const uint32_t c_in = tm.c_in, d_in = tm.d_in;
   const uint64_t nl_base = tm.n_in + st.nl_ex + tm.file_idx;  // slot of my first newline - 1
 
@@ -774,8 +796,23 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
   const uint32_t a_ex = st.dd_ex & 0xFFu, t_ex = (st.dd_ex >> 16) & 0xFFu;
   const int depth0 = int(int8_t(uint8_t(d_in - 1u + (c_in ? (t_ex - a_ex) : a_ex))));
 
-  store2(P.S + F.s_off, lw0, W, S0, S1);
-  if (F.levels > 0) {
+  uint64_t *const S_tile = tm.S_tile, *const LB_tile = tm.LB_tile;
+  // A row of two words, inside the file: one 16-byte store where aligned.
+  auto put2 = [tid](uint64_t *row, bool aligned, uint64_t a, uint64_t b) {
+    if (aligned) {
+      *reinterpret_cast<ulonglong2 *>(row + 2 * tid) = make_ulonglong2(a, b);
+    } else {
+      row[2 * tid] = a;
+      row[2 * tid + 1] = b;
+    }
+  };
+  const bool inside = (flags & kTileInside) != 0;
+  if (inside) {
+    put2(S_tile, (flags & kTileSAligned) != 0, S0, S1);
+  } else {
+    store2(S_tile - tm.lw_tile, lw0, W, S0, S1);
+  }
+  if (levels > 0) {
     uint64_t lb0[LMAX], lb1[LMAX];
     const uint64_t O0 = st.op0 & ~S0, C0 = st.cl0 & ~S0, P0 = st.sp0 & ~S0;
     const uint64_t O1 = st.op1 & ~S1, C1 = st.cl1 & ~S1, P1 = st.sp1 & ~S1;
@@ -785,9 +822,18 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
       const int depth1 = leveled_word<LMAX>(O0, C0, P0, depth0, lb0);
       leveled_word<LMAX>(O1, C1, P1, depth1, lb1);
     }
+    if (inside) {
 #pragma unroll
-    for (int l = 0; l < LMAX; ++l) {
-      if (l < F.levels) store2(P.LB + F.lb_off + uint64_t(l) * W, lw0, W, lb0[l], lb1[l]);
+      for (int l = 0; l < LMAX; ++l) {
+        if (l < levels)
+          put2(LB_tile + uint64_t(l) * W, ((flags >> (kTileLevelAligned + l)) & 1u) != 0, lb0[l],
+               lb1[l]);
+      }
+    } else {
+#pragma unroll
+      for (int l = 0; l < LMAX; ++l) {
+        if (l < levels) store2(LB_tile - tm.lw_tile + uint64_t(l) * W, lw0, W, lb0[l], lb1[l]);
+      }
     }
   }
   // newline offsets (every '\n' counts, strings or not), file-local
