@@ -345,13 +345,14 @@ struct TileMeta {  // a tile between its phase A and its phase B
   // words from the tile's first word on, the file's word count and the
   // tile's first word.  store_flags: kTileInside when every word of the
   // tile lies inside the file (the stores need no bounds check), kTileSAligned
-  // when the S row of every thread starts on 16 bytes, and bit
-  // kTileLevelAligned + l when level l's rows do.
+  // when the S row of every thread starts on 16 bytes, bit kTileLevelAligned
+  // + l when level l's rows do, and kTileAllAligned when all of them do.
   uint64_t *S_tile, *LB_tile;
   uint64_t W, lw_tile;
   uint32_t store_flags;
 };
-constexpr uint32_t kTileInside = 1u, kTileSAligned = 2u, kTileLevelAligned = 8u;
+constexpr uint32_t kTileInside = 1u, kTileSAligned = 2u, kTileAllAligned = 4u,
+                   kTileLevelAligned = 8u;
 
 template <int NT>
 struct PipeSmem {
@@ -371,10 +372,18 @@ struct PipeSmem {
 // touches the slots of its own two words.  Level LMAX is a sink for the
 // masks of depths that are not stored, so the walk writes without a branch.
 constexpr int kSharedLevels = 8;  // LMAX up to this stages in shared memory
+// Indexes of up to four levels walk quarters with two or more bracket
+// events from a per-warp list (every lane takes one), the rest in the lane
+// that owns them.
+template <int LMAX>
+__host__ __device__ constexpr bool walk_list() {
+  return LMAX <= 4;
+}
 template <int NT, int LMAX>
 struct LevelScratch {
   static constexpr int NW = NT / 32;
   uint64_t lb[NW][LMAX + 1][64];
+  uint4 items[walk_list<LMAX>() ? NW : 1][128];  // O, C, P, start depth | quarter << 8
 };
 
 // One thread's row between phase A and phase B.
@@ -691,10 +700,14 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
     tm.LB_tile = P.LB + F.lb_off + lw_tile;
     uint32_t flags = lw_tile + 2u * NT <= W ? kTileInside : 0u;
     if ((reinterpret_cast<uintptr_t>(tm.S_tile) & 15u) == 0) flags |= kTileSAligned;
-    for (int l = 0; l < F.levels && l < 24; ++l)
+    bool all = (flags & kTileSAligned) != 0;
+    for (int l = 0; l < F.levels && l < 24; ++l) {
       if ((reinterpret_cast<uintptr_t>(tm.LB_tile + uint64_t(l) * W) & 15u) == 0)
         flags |= 1u << (kTileLevelAligned + l);
-    tm.store_flags = flags;
+      else
+        all = false;
+    }
+    tm.store_flags = flags | (all ? kTileAllAligned : 0u);
     mbar_arrive(smem_u32(&sm.agg[k & 1u]));
   }
   st.op0 = c0.op;
@@ -738,6 +751,57 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
   // .. LMAX-1 are the bytes 0 .. LMAX-1, negative depths the bytes 128 ..
   // 255, and every byte from LMAX up selects the sink level.
   uint32_t d = uint32_t(depth0);
+  if constexpr (walk_list<LMAX>()) {
+    // A quarter with at most one event takes two masks, written here; a
+    // quarter with more goes to the warp's list, ordered by quarter then
+    // lane, and each lane walks one listed quarter per pass.  A warp then
+    // iterates about as often as its busiest listed quarter needs, not as
+    // often as its busiest lane needs in each of the four quarters.  Every
+    // (level, quarter) slot has one writer: the owner or the lane walking it.
+    uint32_t *wslot = reinterpret_cast<uint32_t *>(&ls.lb[warp][0][0]);  // [level * 128 + q]
+    uint4 *items = ls.items[warp];
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t listed = 0;
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const uint64_t Ow = h < 2 ? O0 : O1, Cw = h < 2 ? C0 : C1, Pw = h < 2 ? P0 : P1;
+      const uint32_t O = uint32_t((h & 1) ? (Ow >> 32) : Ow);
+      const uint32_t C = uint32_t((h & 1) ? (Cw >> 32) : Cw);
+      const uint32_t Pm = uint32_t((h & 1) ? (Pw >> 32) : Pw);
+      const uint32_t PO = Pm | O, ev = O | C;
+      const uint32_t q = uint32_t(lane) * 4u + uint32_t(h);
+      const bool heavy = (ev & (ev - 1u)) != 0u;
+      const uint32_t hb = __ballot_sync(0xFFFFFFFFu, heavy);
+      if (heavy) {
+        items[listed + __popc(hb & lt)] = make_uint4(O, C, Pm, (d & 0xFFu) | (q << 8));
+      } else {
+        // bit: the event, or 0 (below then covers the whole quarter)
+        const uint32_t bit = ev & (0u - ev);
+        const uint32_t below = bit - 1u;
+        wslot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + q] |= (below & PO) | (bit & ~O);
+        const uint32_t d1 = d + ((O & bit) ? 1u : (bit ? 0xFFFFFFFFu : 0u));
+        wslot[min(d1 & 0xFFu, uint32_t(LMAX)) * 128 + q] |= PO & ~below;
+      }
+      listed += __popc(hb);
+      d += uint32_t(__popc(O)) - uint32_t(__popc(C));
+    }
+    __syncwarp();
+    for (uint32_t i = uint32_t(lane); i < listed; i += 32u) {
+      const uint4 it = items[i];
+      const uint32_t O = it.x, C = it.y, PO = it.z | it.x, q = it.w >> 8;
+      uint32_t dq = it.w, ev = O | C, below_prev = 0u;
+      while (ev) {  // as below
+        const uint32_t bit = ev & (0u - ev);
+        const uint32_t below = bit - 1u;
+        wslot[min(dq & 0xFFu, uint32_t(LMAX)) * 128 + q] |= ((below ^ below_prev) & PO) | (bit & ~O);
+        dq += (O & bit) ? 1u : 0xFFFFFFFFu;
+        below_prev = below;
+        ev ^= bit;
+      }
+      wslot[min(dq & 0xFFu, uint32_t(LMAX)) * 128 + q] |= PO & ~below_prev;
+    }
+    __syncwarp();
+  } else {
 #pragma unroll
   for (int h = 0; h < 4; ++h) {
     const uint64_t Ow = h < 2 ? O0 : O1, Cw = h < 2 ? C0 : C1, Pw = h < 2 ? P0 : P1;
@@ -762,6 +826,7 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
     }
     // the run after the quarter's last event
     slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= PO & ~below_prev;
+  }
   }
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
@@ -822,7 +887,14 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
       const int depth1 = leveled_word<LMAX>(O0, C0, P0, depth0, lb0);
       leveled_word<LMAX>(O1, C1, P1, depth1, lb1);
     }
-    if (inside) {
+    if (inside && (flags & kTileAllAligned) != 0) {
+#pragma unroll
+      for (int l = 0; l < LMAX; ++l) {
+        if (l < levels)
+          *reinterpret_cast<ulonglong2 *>(LB_tile + uint64_t(l) * W + 2 * tid) =
+              make_ulonglong2(lb0[l], lb1[l]);
+      }
+    } else if (inside) {
 #pragma unroll
       for (int l = 0; l < LMAX; ++l) {
         if (l < levels)
