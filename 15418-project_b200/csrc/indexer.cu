@@ -726,14 +726,14 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
   st.nl_ex = nl_ex;
 }
 
-// Leveled bitmaps of one lane's two words, walked as one event sequence in
-// 32-bit quarters (word 0 low, word 0 high, word 1 low, word 1 high, the
-// depth carried over), so every step is 32-bit integer work and a warp
-// iterates as often as its busiest lane has events in its row.  Separators
-// between two events share one depth; an opening bracket belongs to the
-// level it opens, a closing one to the level it closes (signed-char depth,
-// sharemem/leveled-bitmaps-index.cu:270-300).  Each mask is OR-ed into the
-// lane's own shared-memory slot of its level and quarter.
+// Leveled bitmaps of one lane's two words, walked as event sequences in
+// 32-bit quarters (word 0 low, word 0 high, word 1 low, word 1 high; each
+// quarter starts at the depth the quarters before it leave), so every step
+// is 32-bit integer work.  Separators between two events share one depth;
+// an opening bracket belongs to the level it opens, a closing one to the
+// level it closes (signed-char depth, sharemem/leveled-bitmaps-index.cu:
+// 270-300).  Each mask is OR-ed into the shared-memory slot of its level and
+// quarter; the lane reads its two words' slots back once all are written.
 template <int LMAX, int NT>
 __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_t O0,
                                              uint64_t C0, uint64_t P0, uint64_t O1, uint64_t C1,
@@ -790,7 +790,7 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
       const uint4 it = items[i];
       const uint32_t O = it.x, C = it.y, PO = it.z | it.x, q = it.w >> 8;
       uint32_t dq = it.w, ev = O | C, below_prev = 0u;
-      while (ev) {  // as below
+      while (ev) {  // the walk of the per-lane loop below
         const uint32_t bit = ev & (0u - ev);
         const uint32_t below = bit - 1u;
         wslot[min(dq & 0xFFu, uint32_t(LMAX)) * 128 + q] |= ((below ^ below_prev) & PO) | (bit & ~O);
@@ -803,30 +803,30 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
     __syncwarp();
   } else {
 #pragma unroll
-  for (int h = 0; h < 4; ++h) {
-    const uint64_t Ow = h < 2 ? O0 : O1, Cw = h < 2 ? C0 : C1, Pw = h < 2 ? P0 : P1;
-    const uint32_t O = uint32_t((h & 1) ? (Ow >> 32) : Ow);
-    const uint32_t C = uint32_t((h & 1) ? (Cw >> 32) : Cw);
-    const uint32_t Pm = uint32_t((h & 1) ? (Pw >> 32) : Pw);
-    // Between two consecutive events the only bits of P | O are the
-    // separators and, when the earlier event opens a level, its own bit:
-    // exactly the bits of that run's level.
-    const uint32_t PO = Pm | O;
-    uint32_t ev = O | C, below_prev = 0u;
-    while (ev) {  // branch-free body: lanes only differ in the trip count
-      const uint32_t bit = ev & (0u - ev);
-      const uint32_t below = bit - 1u;
-      // the run since the last event, and a closing bracket, which joins
-      // the level it closes
-      const uint32_t m = ((below ^ below_prev) & PO) | (bit & ~O);
-      slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= m;
-      d += (O & bit) ? 1u : 0xFFFFFFFFu;
-      below_prev = below;
-      ev ^= bit;
+    for (int h = 0; h < 4; ++h) {
+      const uint64_t Ow = h < 2 ? O0 : O1, Cw = h < 2 ? C0 : C1, Pw = h < 2 ? P0 : P1;
+      const uint32_t O = uint32_t((h & 1) ? (Ow >> 32) : Ow);
+      const uint32_t C = uint32_t((h & 1) ? (Cw >> 32) : Cw);
+      const uint32_t Pm = uint32_t((h & 1) ? (Pw >> 32) : Pw);
+      // Between two consecutive events the only bits of P | O are the
+      // separators and, when the earlier event opens a level, its own bit:
+      // exactly the bits of that run's level.
+      const uint32_t PO = Pm | O;
+      uint32_t ev = O | C, below_prev = 0u;
+      while (ev) {  // branch-free body: lanes only differ in the trip count
+        const uint32_t bit = ev & (0u - ev);
+        const uint32_t below = bit - 1u;
+        // the run since the last event, and a closing bracket, which joins
+        // the level it closes
+        const uint32_t m = ((below ^ below_prev) & PO) | (bit & ~O);
+        slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= m;
+        d += (O & bit) ? 1u : 0xFFFFFFFFu;
+        below_prev = below;
+        ev ^= bit;
+      }
+      // the run after the quarter's last event
+      slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= PO & ~below_prev;
     }
-    // the run after the quarter's last event
-    slot[min(d & 0xFFu, uint32_t(LMAX)) * 128 + h] |= PO & ~below_prev;
-  }
   }
 #pragma unroll
   for (int l = 0; l < LMAX; ++l) {
