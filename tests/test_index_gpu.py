@@ -79,6 +79,29 @@ def test_levels(cuda_ctx, gpj, levels):
     assert_same(gpu_index(cuda_ctx, gpj, data, levels), oracle.OracleIndex(data, levels))
 
 
+@pytest.mark.parametrize("levels", [1, 2, 4])
+def test_listed_walk_dense_and_sparse_quarters(cuda_ctx, gpj, levels):
+    """Indexes of up to four levels walk the 32-byte quarters that hold two
+    or more brackets from a per-warp list and the others straight-line:
+    bracket-dense runs (every quarter of a warp listed, four passes) next to
+    sparse records (empty and single-event quarters), and bracket runs deep
+    enough to wrap the signed-char depth inside listed quarters."""
+    rng = random.Random(100 + levels)
+    parts = []
+    for _ in range(80):
+        k = rng.randrange(4)
+        if k == 0:
+            parts.append(b"[" * rng.randrange(1, 300))
+        elif k == 1:
+            parts.append(b"]" * rng.randrange(1, 300))
+        elif k == 2:
+            parts.append(bytes(rng.choices(b"{}[]:,", k=rng.randrange(100, 5000))))
+        else:
+            parts.append(b'{"a":1,"b":"x' + b" " * rng.randrange(0, 3000) + b'"}\n')
+    data = b"".join(parts)
+    assert_same(gpu_index(cuda_ctx, gpj, data, levels), oracle.OracleIndex(data, levels))
+
+
 @pytest.mark.parametrize("offset", [1, 3, 8, 13])
 def test_unaligned_input(cuda_ctx, gpj, offset):
     rng = random.Random(offset)
