@@ -64,6 +64,8 @@ STAGE_INDEX, STAGE_FINALIZE, STAGE_QUERY = 1, 2, 4
 
 GPJ_BATCH_AUTOTUNE = 4
 GPJ_BATCH_NO_GRAPH = 8
+GPJ_BATCH_INDEX_LANE_WALK = 16
+GPJ_BATCH_INDEX_WIDE_LOOKBACK = 32
 FILE_INFO_WORDS = 8  # lines, newline slot, first record, first result int, in-string, depth, bytes, query
 
 
@@ -161,7 +163,7 @@ class BatchView(C.Structure):
                 ("string_words", C.c_uint64), ("leveled_words", C.c_uint64),
                 ("num_tiles", C.c_uint32), ("index_threads", C.c_uint32),
                 ("query_block", C.c_uint32), ("query_grid", C.c_uint32),
-                ("uses_graph", C.c_uint32), ("reserved", C.c_uint32)]
+                ("uses_graph", C.c_uint32), ("index_variant", C.c_uint32)]
 
 
 GPJ_SERVER_NO_CACHE = 1

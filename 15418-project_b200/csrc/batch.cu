@@ -255,6 +255,8 @@ int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
   b->input_bytes = input_bytes;
   b->num_files = num_files;
   b->flags = flags;
+  b->L.variant = ((flags & GPJ_BATCH_INDEX_LANE_WALK) ? gpjb::kIndexVariantLaneWalk : 0u) |
+                 ((flags & GPJ_BATCH_INDEX_WIDE_LOOKBACK) ? gpjb::kIndexVariantWideLookback : 0u);
   // query groups: IR packed into one 4 KiB blob
   int ir_off = 0;
   std::vector<uint32_t> slots(num_queries);
@@ -341,25 +343,29 @@ int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
   b->query_grid = sms * 8;
 
   if (flags & GPJ_BATCH_AUTOTUNE) {
-    // launch shapes: indexer tile (128 or 256 threads x 128 B), query block
-    // and persistent grid; each candidate is timed over a few runs
+    // Two stages, each candidate timed over a few runs of the whole chain.
+    // First the indexer: tile size (128 or 256 threads x 128 B) and kernel
+    // variant (listed or per-lane leveled walk, look-back rounds of 32 or
+    // 64 descriptors), with the default query shape.  Then the query block
+    // and persistent grid for that indexer.
     float best = 1e30f;
-    int best_t = b->index_threads, best_b = b->query_block, best_g = b->query_grid;
+    int best_t = b->index_threads;
+    uint32_t best_v = b->L.variant;
     for (int threads : {256, 128}) {
       layout(b, threads);
       b->index_threads = threads;
       if ((rc = alloc_layout_buffers(b)) != GPJ_OK) return bail(rc);
-      for (int block : {128, 256}) {
-        for (int gm : {4, 5, 8, 16}) {
-          b->query_block = block;
-          b->query_grid = sms * gm * (256 / block);
-          const float ms = time_chain(b, s, 3);
-          if (ms < best) {
-            best = ms;
-            best_t = threads;
-            best_b = block;
-            best_g = b->query_grid;
-          }
+      const uint32_t variants[] = {0u, uint32_t(gpjb::kIndexVariantLaneWalk),
+                                   uint32_t(gpjb::kIndexVariantWideLookback),
+                                   uint32_t(gpjb::kIndexVariantLaneWalk) |
+                                       uint32_t(gpjb::kIndexVariantWideLookback)};
+      for (uint32_t variant : variants) {
+        b->L.variant = variant;
+        const float ms = time_chain(b, s, 3);
+        if (ms < best) {
+          best = ms;
+          best_t = threads;
+          best_v = variant;
         }
       }
     }
@@ -367,6 +373,21 @@ int gpj_batch_create(gpj_ctx *ctx, const uint8_t *d_input, uint64_t input_bytes,
       layout(b, best_t);
       b->index_threads = best_t;
       if ((rc = alloc_layout_buffers(b)) != GPJ_OK) return bail(rc);
+    }
+    b->L.variant = best_v;
+    best = 1e30f;
+    int best_b = b->query_block, best_g = b->query_grid;
+    for (int block : {128, 256}) {
+      for (int gm : {4, 5, 8, 16}) {
+        b->query_block = block;
+        b->query_grid = sms * gm * (256 / block);
+        const float ms = time_chain(b, s, 3);
+        if (ms < best) {
+          best = ms;
+          best_b = block;
+          best_g = b->query_grid;
+        }
+      }
     }
     b->query_block = best_b;
     b->query_grid = best_g;
@@ -591,6 +612,7 @@ int gpj_batch_view_get(const gpj_batch *b, gpj_batch_view *v) {
   v->query_block = uint32_t(b->query_block);
   v->query_grid = uint32_t(b->query_grid);
   v->uses_graph = b->exec != nullptr ? 1u : 0u;
+  v->index_variant = b->L.variant;
   return GPJ_OK;
 }
 

@@ -42,13 +42,13 @@ __device__ __forceinline__ void st_relaxed(unsigned long long *p, uint64_t v) {
 constexpr uint32_t kSpinLimit = 1u << 22;
 
 // One warp.  Walks back over the predecessors of `tile` (whose own aggregate
-// is already published), 32 per round (one descriptor per lane, loaded
+// is already published), 32 * K per round (K descriptors per lane, loaded
 // together so one round costs one memory round trip), and returns the tile's
 // exclusive prefix.  The fold works on packed descriptors: two shuffles and
-// one branch-free composition per step.  Rounds of 32 were measured faster
-// than rounds of 64 or 128: a nearby inclusive descriptor is the usual case,
-// and fewer polled lines wait on fewer unpublished tiles.
-constexpr int kLookbackPerLane = 1;
+// one branch-free composition per step.  Rounds of 32 (K = 1) were measured
+// faster than rounds of 64 or 128 on the configured workloads: a nearby
+// inclusive descriptor is the usual case, and fewer polled lines wait on
+// fewer unpublished tiles; the batch autotuner also tries K = 2.
 
 __device__ __forceinline__ uint64_t shfl_down_u64(uint64_t v, int off) {
   const uint32_t lo = __shfl_down_sync(0xFFFFFFFFu, uint32_t(v), off);
@@ -61,6 +61,7 @@ __device__ __forceinline__ uint64_t shfl_u64(uint64_t v, int src) {
   return (uint64_t(hi) << 32) | lo;
 }
 
+template <int kLookbackPerLane>
 __device__ Agg lookback(const IndexLaunch &P, uint32_t tile) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) return agg_identity();
@@ -372,18 +373,18 @@ struct PipeSmem {
 // touches the slots of its own two words.  Level LMAX is a sink for the
 // masks of depths that are not stored, so the walk writes without a branch.
 constexpr int kSharedLevels = 8;  // LMAX up to this stages in shared memory
-// Indexes of up to four levels walk quarters with two or more bracket
+// Indexes of up to four levels can walk quarters with two or more bracket
 // events from a per-warp list (every lane takes one), the rest in the lane
-// that owns them.
+// that owns them (kList); otherwise every lane walks its own four quarters.
 template <int LMAX>
-__host__ __device__ constexpr bool walk_list() {
+__host__ __device__ constexpr bool walk_list_allowed() {
   return LMAX <= 4;
 }
-template <int NT, int LMAX>
+template <int NT, int LMAX, bool kList>
 struct LevelScratch {
   static constexpr int NW = NT / 32;
   uint64_t lb[NW][LMAX + 1][64];
-  uint4 items[walk_list<LMAX>() ? NW : 1][128];  // O, C, P, start depth | quarter << 8
+  uint4 items[kList ? NW : 1][128];  // O, C, P, start depth | quarter << 8
 };
 
 // One thread's row between phase A and phase B.
@@ -513,8 +514,9 @@ __device__ __forceinline__ void control_fill(const IndexLaunch &P, PipeSmem<NT> 
   tile_out = t;
 }
 
-template <int NT, bool kTma>
+template <int NT, bool kTma, int kLB>
 __device__ void control_warp(const IndexLaunch &P, PipeSmem<NT> &sm, const CUtensorMap *tmap) {
+  static_assert(kLB == 1 || kLB == 2, "look-back descriptors per lane");
   const int lane = threadIdx.x & 31;
   const volatile uint32_t *abort = &sm.abort;
   uint32_t stage_tile[kStages] = {kEndTile, kEndTile};
@@ -542,7 +544,7 @@ __device__ void control_warp(const IndexLaunch &P, PipeSmem<NT> &sm, const CUten
     const IndexFile F = tm.F;
     const bool file_start = tile == F.first_tile;
     const Agg local = tile_aggregate(tm.par, tm.dd, tm.nl, file_start);
-    const Agg prefix = lookback(P, tile);
+    const Agg prefix = lookback<kLB>(P, tile);
     if (lane == 0) {
       const Agg incl = agg_combine(prefix, local);
       st_relaxed(&P.tile_state[tile], agg_pack(kStatusIncl, incl));
@@ -734,8 +736,8 @@ __device__ __forceinline__ void phase_a(const IndexLaunch &P, PipeSmem<NT> &sm, 
 // level it closes (signed-char depth, sharemem/leveled-bitmaps-index.cu:
 // 270-300).  Each mask is OR-ed into the shared-memory slot of its level and
 // quarter; the lane reads its two words' slots back once all are written.
-template <int LMAX, int NT>
-__device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_t O0,
+template <int LMAX, int NT, bool kList>
+__device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX, kList> &ls, uint64_t O0,
                                              uint64_t C0, uint64_t P0, uint64_t O1, uint64_t C1,
                                              uint64_t P1, int depth0, uint64_t (&lb0)[LMAX],
                                              uint64_t (&lb1)[LMAX]) {
@@ -751,7 +753,7 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
   // .. LMAX-1 are the bytes 0 .. LMAX-1, negative depths the bytes 128 ..
   // 255, and every byte from LMAX up selects the sink level.
   uint32_t d = uint32_t(depth0);
-  if constexpr (walk_list<LMAX>()) {
+  if constexpr (kList) {
     // A quarter with at most one event takes two masks, written here; a
     // quarter with more goes to the warp's list, ordered by quarter then
     // lane, and each lane walks one listed quarter per pass.  A warp then
@@ -835,9 +837,9 @@ __device__ __forceinline__ void leveled_lane(LevelScratch<NT, LMAX> &ls, uint64_
   }
 }
 
-template <int LMAX, int NT>
+template <int LMAX, int NT, bool kList>
 __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
-                                        LevelScratch<NT, LMAX> &ls, uint32_t k,
+                                        LevelScratch<NT, LMAX, kList> &ls, uint32_t k,
                                         const RowState &st) {
   const int tid = threadIdx.x;
   const int j = int(k & 1u);
@@ -882,7 +884,7 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
     const uint64_t O0 = st.op0 & ~S0, C0 = st.cl0 & ~S0, P0 = st.sp0 & ~S0;
     const uint64_t O1 = st.op1 & ~S1, C1 = st.cl1 & ~S1, P1 = st.sp1 & ~S1;
     if constexpr (LMAX <= kSharedLevels) {
-      leveled_lane<LMAX, NT>(ls, O0, C0, P0, O1, C1, P1, depth0, lb0, lb1);
+      leveled_lane<LMAX, NT, kList>(ls, O0, C0, P0, O1, C1, P1, depth0, lb0, lb1);
     } else {
       const int depth1 = leveled_word<LMAX>(O0, C0, P0, depth0, lb0);
       leveled_word<LMAX>(O1, C1, P1, depth1, lb1);
@@ -926,15 +928,18 @@ __device__ __forceinline__ void phase_b(const IndexLaunch &P, PipeSmem<NT> &sm,
   }
 }
 
-template <int LMAX, bool kTma, int NT>
+// LMAX: levels the kernel can store; kTma: tiles staged by TMA; NT: compute
+// threads; kList: the listed leveled walk; kLB: look-back descriptors per
+// lane.
+template <int LMAX, bool kTma, int NT, bool kList, int kLB>
 __global__ void __launch_bounds__(NT + 32, LMAX > 8 ? 1 : (NT <= 128 ? 4 : 2))
     index_kernel(const __grid_constant__ CUtensorMap tmap, const IndexLaunch P) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // the 128-byte-swizzled TMA destinations need 1024-byte alignment
   uint8_t *smem_base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   PipeSmem<NT> &sm = *reinterpret_cast<PipeSmem<NT> *>(smem_base);
-  LevelScratch<NT, LMAX> &ls =
-      *reinterpret_cast<LevelScratch<NT, LMAX> *>(smem_base + level_scratch_offset<NT>());
+  LevelScratch<NT, LMAX, kList> &ls = *reinterpret_cast<LevelScratch<NT, LMAX, kList> *>(
+      smem_base + level_scratch_offset<NT>());
   const int tid = threadIdx.x;
   if (tid == NT) {
     // barriers must be initialised before anyone polls them: shared memory
@@ -954,7 +959,7 @@ __global__ void __launch_bounds__(NT + 32, LMAX > 8 ? 1 : (NT <= 128 ? 4 : 2))
   }
   __syncthreads();
   if (tid >= NT) {
-    control_warp<NT, kTma>(P, sm, &tmap);
+    control_warp<NT, kTma, kLB>(P, sm, &tmap);
     return;
   }
   RowState prev{};
@@ -973,18 +978,18 @@ __global__ void __launch_bounds__(NT + 32, LMAX > 8 ? 1 : (NT <= 128 ? 4 : 2))
     if (stop) break;
     RowState cur;
     phase_a<LMAX, kTma, NT>(P, sm, s, k, cur);
-    if (k > 0) phase_b<LMAX, NT>(P, sm, ls, k - 1, prev);
+    if (k > 0) phase_b<LMAX, NT, kList>(P, sm, ls, k - 1, prev);
     prev = cur;
   }
   if (k > 0 && !*static_cast<volatile uint32_t *>(&sm.abort))
-    phase_b<LMAX, NT>(P, sm, ls, k - 1, prev);
+    phase_b<LMAX, NT, kList>(P, sm, ls, k - 1, prev);
 }
 
-template <int LMAX, bool kTma, int NT>
+template <int LMAX, bool kTma, int NT, bool kList, int kLB>
 cudaError_t launch_kernel(const IndexLaunch &L, const CUtensorMap &map, cudaStream_t stream) {
-  auto kernel = index_kernel<LMAX, kTma, NT>;
+  auto kernel = index_kernel<LMAX, kTma, NT, kList, kLB>;
   constexpr size_t smem = level_scratch_offset<NT>() +
-                          (LMAX <= kSharedLevels ? sizeof(LevelScratch<NT, LMAX>) : 0) +
+                          (LMAX <= kSharedLevels ? sizeof(LevelScratch<NT, LMAX, kList>) : 0) +
                           1024;  // + alignment slack
   static int grid_per_device[64] = {};
   int dev = 0;
@@ -1007,12 +1012,30 @@ cudaError_t launch_kernel(const IndexLaunch &L, const CUtensorMap &map, cudaStre
   return cudaGetLastError();
 }
 
+template <int LMAX, int NT, bool kList, int kLB>
+cudaError_t launch_tma(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
+                       cudaStream_t stream) {
+  if (use_tma) return launch_kernel<LMAX, true, NT, kList, kLB>(L, *map, stream);
+  CUtensorMap dummy{};
+  return launch_kernel<LMAX, false, NT, kList, kLB>(L, dummy, stream);
+}
+
+// The launch variant (IndexLaunch::variant) picks the walk and the look-back
+// granularity where both forms exist (up to four levels); deeper indexes
+// always walk per lane with rounds of 32 descriptors.
 template <int LMAX, int NT>
 cudaError_t launch_levels(const IndexLaunch &L, const CUtensorMap *map, bool use_tma,
                           cudaStream_t stream) {
-  if (use_tma) return launch_kernel<LMAX, true, NT>(L, *map, stream);
-  CUtensorMap dummy{};
-  return launch_kernel<LMAX, false, NT>(L, dummy, stream);
+  if constexpr (walk_list_allowed<LMAX>()) {
+    const bool lanes = (L.variant & kIndexVariantLaneWalk) != 0;
+    const bool wide = (L.variant & kIndexVariantWideLookback) != 0;
+    if (lanes && wide) return launch_tma<LMAX, NT, false, 2>(L, map, use_tma, stream);
+    if (lanes) return launch_tma<LMAX, NT, false, 1>(L, map, use_tma, stream);
+    if (wide) return launch_tma<LMAX, NT, true, 2>(L, map, use_tma, stream);
+    return launch_tma<LMAX, NT, true, 1>(L, map, use_tma, stream);
+  } else {
+    return launch_tma<LMAX, NT, false, 1>(L, map, use_tma, stream);
+  }
 }
 
 template <int NT>

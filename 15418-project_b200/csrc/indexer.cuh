@@ -57,6 +57,15 @@ struct IndexLaunch {
   uint32_t tile_begin = 0, tile_end = 0;
   // polls after which a look-back gives up on an unpublished predecessor
   uint32_t lookback_spin_limit = 1u << 22;
+  // kernel variant (kIndexVariant* bits; 0 = default), chosen by the batch
+  // autotuner; the outputs are the same for every variant
+  uint32_t variant = 0;
+};
+
+// Index kernel variants for indexes of up to four levels.
+enum : uint32_t {
+  kIndexVariantLaneWalk = 1u,      // every lane walks its own quarters (no list)
+  kIndexVariantWideLookback = 2u,  // look-back rounds of 64 descriptors instead of 32
 };
 
 // Error bits the kernels raise in IndexLaunch::error.

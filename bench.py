@@ -824,6 +824,8 @@ def run_batch(args, world, rank, local):
         "config": {"workload": C3_DESC, "input_bytes": total, "files": len(files), "records": int(v.num_records),
                    "l2": "input larger than L2", "parallelism": f"file shards x{world}",
                    "launch_shape": {"index_threads": v.index_threads,
+                                    "index_walk": ("per-lane" if v.index_variant & 1 else "listed"),
+                                    "lookback_descriptors": 64 if v.index_variant & 2 else 32,
                                     "query_block": v.query_block, "query_grid": v.query_grid,
                                     "graph": bool(v.uses_graph)}},
         "plain_per_file": {"value": round(gb / (ms_plain / 1e3), 3), "unit": "GB/s",

@@ -273,8 +273,13 @@ int gpj_results_compact(gpj_ctx *ctx, const int32_t *d_results, uint64_t num_lin
 /* Batched path: many files indexed and queried by one launch chain         */
 /* ------------------------------------------------------------------------ */
 
-#define GPJ_BATCH_AUTOTUNE 4u /* time the launch shapes at creation, keep the fastest */
+#define GPJ_BATCH_AUTOTUNE 4u /* time the launch shapes at creation, keep the fastest: indexer
+                                 tile size and variant, then query block and grid */
 #define GPJ_BATCH_NO_GRAPH 8u /* launch the kernels directly instead of a CUDA graph */
+/* Indexer variant without GPJ_BATCH_AUTOTUNE (gpj_batch_view.index_variant;
+ * indexes of up to 4 levels, same outputs): */
+#define GPJ_BATCH_INDEX_LANE_WALK 16u      /* each lane walks its own leveled quarters */
+#define GPJ_BATCH_INDEX_WIDE_LOOKBACK 32u  /* look-back rounds of 64 descriptors */
 
 /* One file of a batch: `offset` (a multiple of 128) and `size_bytes` inside
  * the batch's device buffer; `query` indexes the batch's query table. */
@@ -323,7 +328,9 @@ typedef struct gpj_batch_view {
   uint32_t query_block;
   uint32_t query_grid;
   uint32_t uses_graph;
-  uint32_t reserved;
+  uint32_t index_variant; /* indexer variant bits for up to 4 levels: 1 = each lane walks its
+                             own leveled quarters (no per-warp list), 2 = look-back rounds of
+                             64 descriptors (else 32); the outputs are the same for all */
 } gpj_batch_view;
 
 typedef struct gpj_batch gpj_batch;

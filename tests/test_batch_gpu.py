@@ -50,7 +50,8 @@ def _run_batch(gpj, files, flags, runs=1):
         totals = d2h(v.d_totals, 4, np.uint64)
         out = {
             "info": info, "totals": totals, "view": (v.num_records, v.result_ints, v.uses_graph,
-                                                     v.index_threads, v.query_block),
+                                                     v.index_threads, v.query_block,
+                                                     v.index_variant),
             "S": d2h(v.d_string, v.string_words, np.uint64),
             "LB": d2h(v.d_leveled, v.leveled_words, np.uint64),
             "NL": d2h(v.d_newline, v.newline_slots, np.int64),
@@ -99,6 +100,23 @@ def test_batch_without_graph_and_autotuned(gpj):
     _check(files, comp, queries, a)
     _check(files, comp, queries, b)
     assert b["view"][3] in (128, 256) and b["view"][4] in (128, 256)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_batch_index_variants(gpj, variant):
+    """Every indexer variant the batch autotuner chooses among (leveled walk
+    from a per-warp list or per lane, look-back rounds of 32 or 64
+    descriptors) gives the oracle's outputs file by file; a 3 MiB file makes
+    the look-back cross more than 64 tiles."""
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    from gpjson_b200 import datagen
+    flags = ((gpj.GPJ_BATCH_INDEX_LANE_WALK if variant & 1 else 0) |
+             (gpj.GPJ_BATCH_INDEX_WIDE_LOOKBACK if variant & 2 else 0))
+    files = _files(10 + variant, 30) + [(bytes(datagen.products(77, 3 << 20)), 1)]
+    comp, queries, got = _run_batch(gpj, files, flags=flags)
+    assert got["view"][5] == variant
+    _check(files, comp, queries, got)
 
 
 def test_batch_single_large_file_equals_plain_build(gpj, cuda_ctx):
