@@ -131,6 +131,7 @@ gpjb::BatchQueryLaunch query_launch_of(const gpj_batch *b) {
   // overflow of extension queries lands in the error word of the totals
   // (written by the finalize kernel just before the query launch)
   q.status = reinterpret_cast<unsigned int *>(b->d_totals + gpjb::kTotError);
+  q.record_counter = reinterpret_cast<unsigned long long *>(b->d_totals + gpjb::kTotRecordCounter);
   q.num_groups = int(b->groups.size());
   for (size_t g = 0; g < b->groups.size(); ++g) q.groups[g] = b->groups[g];
   return q;

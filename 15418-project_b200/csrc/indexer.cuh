@@ -138,7 +138,13 @@ enum FileInfoField : int {
 };
 
 // Totals of a multi-file build: [records, result ints, newline slots, error].
-enum TotalField : int { kTotRecords = 0, kTotResultInts = 1, kTotNlSlots = 2, kTotError = 3 };
+enum TotalField : int {
+  kTotRecords = 0,
+  kTotResultInts = 1,
+  kTotNlSlots = 2,
+  kTotError = 3,
+  kTotRecordCounter = 4,  // the batch query's record counter (not a total)
+};
 
 // After index_launch on a file table: derives every file's line count,
 // newline-index slot, record and result offsets (exclusive scans over the

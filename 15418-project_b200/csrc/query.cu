@@ -704,8 +704,24 @@ __global__ void __launch_bounds__(256, 5)
   const LevelState<int32_t> L{ends + threadIdx.x, ends + nlev * blockDim.x + threadIdx.x,
                               int(blockDim.x), nlev};
   const uint64_t records = q.totals[kTotRecords];
+  // Records go to warps 32 at a time from a counter, so a warp whose records
+  // were quick takes more instead of every warp doing the same number of
+  // rounds (the launch ends with its slowest warp); without a counter each
+  // thread strides over the records.
+  const bool fed = q.record_counter != nullptr;
   const uint64_t stride = uint64_t(blockDim.x) * gridDim.x;
-  for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < records; r += stride) {
+  uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (;; r += stride) {
+    if (fed) {
+      unsigned long long base = 0;
+      if ((threadIdx.x & 31u) == 0) base = atomicAdd(q.record_counter, 32ull);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base >= records) break;
+      r = base + (threadIdx.x & 31u);
+      if (r >= records) continue;
+    } else if (r >= records) {
+      break;
+    }
     uint32_t lo = 0, hi = q.num_files;  // file_info[lo].rec_off <= r
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
@@ -827,6 +843,10 @@ cudaError_t batch_query_launch(const BatchQueryLaunch &q, const IrBlob &ir, int 
     ext = ext || query_ir_uses_extensions(ir.bytes + q.groups[g].ir_off, q.groups[g].ir_len);
   }
   const size_t smem = size_t(nlev) * size_t(block) * 8u;
+  if (q.record_counter != nullptr) {
+    const cudaError_t e = cudaMemsetAsync(q.record_counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+  }
   if (ext) batch_query_kernel<true><<<grid, block, smem, stream>>>(q, ir, nlev);
   else batch_query_kernel<false><<<grid, block, smem, stream>>>(q, ir, nlev);
   return cudaGetLastError();

@@ -75,6 +75,9 @@ struct BatchQueryLaunch {
   int32_t *out = nullptr;
   unsigned int *status = nullptr;  // kQueryStatusOverflow is OR-ed here (optional)
   unsigned int *file_status = nullptr;  // or into one word per file (optional, first)
+  // records are handed to warps 32 at a time from this counter, which the
+  // launch zeroes first (optional; without it each thread strides)
+  unsigned long long *record_counter = nullptr;
   int num_groups = 0;
   BatchQueryGroup groups[kMaxBatchGroups];
 };
